@@ -1,0 +1,174 @@
+/*
+ * vite_b200.h -- C ABI of the B200-native Louvain library (libvite_b200.so).
+ *
+ * The whole graph lives on one GPU as one rank: Vite's MPI ghost exchange and
+ * remote community-info messages become reads of device arrays, so the ABI has
+ * no communicator. Ids cross the boundary as int64 and weights as double, the
+ * reference's default 64-bit build (edge.hpp:65-69); on the device ids are
+ * int32 (every graph must have fewer than 2^31 vertices) and all arithmetic on
+ * weights, degrees, gains and modularity stays FP64, evaluated in the
+ * reference's order without fused multiply-adds.
+ *
+ * Every function returns a vg_status; VG_OK is 0. On failure vg_last_error()
+ * names the cause. A context is bound to one device and one CUDA stream; calls
+ * on one context must not overlap (one host thread per context).
+ */
+#ifndef VITE_B200_H
+#define VITE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum vg_status {
+    VG_OK = 0,
+    VG_ERR_ARG = 1,      /* invalid argument (the reference asserts or MPI_Aborts, main.cpp:714-768) */
+    VG_ERR_OOM = 2,      /* device memory or the context's memory budget is exhausted */
+    VG_ERR_CUDA = 3,     /* a CUDA runtime call failed */
+    VG_ERR_TIMEOUT = 4,  /* a bounded device-side wait ran out */
+    VG_ERR_STATE = 5     /* call made in the wrong state (e.g. rebuild before any phase) */
+} vg_status;
+
+typedef struct vg_ctx vg_ctx;
+typedef struct vg_graph vg_graph;
+
+/* Vite's Edge for the default 64-bit build (edge.hpp:72-80): 16 bytes. */
+typedef struct vg_edge {
+    int64_t tail;
+    double weight;
+} vg_edge;
+
+/* Arguments of one Louvain phase: the trailing arguments of the nine
+ * distLouvainMethod* overloads (louvain.hpp:80-137), selected the way main.cpp
+ * dispatches them (main.cpp:267-370). */
+typedef struct vg_phase_params {
+    double lower;       /* `lower`; main passes -1.0 */
+    double threshold;   /* `thresh` */
+    int32_t et_type;    /* 0 plain; 1..4 early termination as -t 1..4 */
+    double et_delta;    /* `ETDelta` (-a), used by types 2 and 4 */
+    int32_t ordering;   /* 0 distLouvainMethod, 1 distLouvainMethodWithColoring,
+                           2 distLouvainMethodVertexOrder (both need vg_color or vg_set_colors) */
+} vg_phase_params;
+
+/* graphClustering's options that shape the phase loop (main.cpp:609-708). */
+typedef struct vg_run_params {
+    double threshold;          /* -h (default 1e-6, utils.hpp:71-73) */
+    int32_t coloring;          /* -c */
+    int32_t vertex_order;      /* -d */
+    int32_t max_colors;        /* the k of -c/-d (default 8) */
+    int32_t single_color_iter; /* the "single" flag of -c/-d */
+    int32_t et_type;           /* -t (0 = off) */
+    double et_delta;           /* -a */
+    int32_t threshold_scaling; /* -i */
+    int32_t one_phase;         /* -p */
+} vg_run_params;
+
+/* What graphClustering prints per level (main.cpp:465-474), measured on the device. */
+typedef struct vg_level_stat {
+    int64_t nv, ne;            /* graph the level ran on */
+    int32_t iters;             /* iterations of the phase */
+    double modularity;         /* value returned by the phase */
+    int64_t num_colors;        /* colors returned by the coloring (0 if none) */
+    double seconds_color;      /* device time of the coloring */
+    double seconds_phase;      /* device time of the phase, coloring excluded */
+    double seconds_sweep;      /* device time of the local-moving sweeps alone */
+    double seconds_rebuild;    /* device time of the rebuild after the level (0 if none) */
+    int64_t edges_swept;       /* sum over iterations of the edges the sweeps visited */
+} vg_level_stat;
+
+/* --- context ---------------------------------------------------------------- */
+
+/* Create a context on `device` with a device-memory budget in bytes (0 = no
+ * budget beyond the device's capacity). Replaces MPI_Init/communicator set-up
+ * (main.cpp:112-118). */
+vg_status vg_ctx_create(int device, size_t mem_budget_bytes, vg_ctx **out);
+vg_status vg_ctx_destroy(vg_ctx *ctx);
+const char *vg_last_error(const vg_ctx *ctx);
+/* Bytes the context currently holds on the device. */
+size_t vg_ctx_bytes_in_use(const vg_ctx *ctx);
+/* Kernel launches issued since the last reset (always counted) and, while
+ * enabled, the sum of their device times in ms (events around each launch). */
+vg_status vg_ctx_profile(vg_ctx *ctx, int32_t enable, double *kernel_ms_out,
+                         int64_t *launches_out, int32_t reset);
+/* The CUDA stream (cudaStream_t) all of the context's work runs on, so callers
+ * can time it with events or order their own work after it. */
+vg_status vg_ctx_stream(vg_ctx *ctx, void **stream_out);
+
+/* --- graphs ----------------------------------------------------------------- */
+
+/* Copy a CSR in Vite's layout (Graph::edgeListIndexes / edgeList,
+ * graph.hpp:77-106) to the device. Replaces loadDistGraphMPIIO's hand-off of
+ * the local graph (distgraph.cpp:119-253) for one rank. */
+vg_status vg_graph_upload(vg_ctx *ctx, int64_t nv, int64_t ne, const int64_t *rowptr,
+                          const vg_edge *edges, vg_graph **out);
+vg_status vg_graph_info(const vg_graph *g, int64_t *nv, int64_t *ne);
+/* Copy the device CSR back in Vite's layout (writeGraph's input,
+ * distgraph.cpp:986-1064). rowptr has nv+1 entries, edges ne. */
+vg_status vg_graph_download(vg_ctx *ctx, const vg_graph *g, int64_t *rowptr, vg_edge *edges);
+vg_status vg_graph_free(vg_ctx *ctx, vg_graph *g);
+
+/* distSumVertexDegree + distCalcConstantForSecondTerm (louvain.cpp:2161-2218):
+ * weighted degree of every vertex (optional copy out) and 1/(2m). */
+vg_status vg_vertex_degree(vg_ctx *ctx, vg_graph *g, double *vdeg_out, double *constant_out);
+
+/* --- the Louvain path ----------------------------------------------------------- */
+
+/* One Louvain phase: distLouvainMethod / ...WithColoring / ...VertexOrder
+ * (louvain.cpp:7-1938). Returns the phase's modularity (`prevMod` of the
+ * reference), its iteration count and, if cvect_out is not NULL, the community
+ * of every vertex (`cvect`). The communities also stay on the device for
+ * vg_rebuild. */
+vg_status vg_louvain_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p,
+                           int64_t *cvect_out, double *mod_out, int32_t *iters_out);
+
+/* distColoringMultiHashMinMax (coloring.cpp:52-118) for one rank: n_hash hash
+ * functions, stop at target_percent coverage or after one round. Returns the
+ * reference's return value (`nextColor`, main passes it +1 as numColor) and
+ * optionally every vertex's color (-1 = uncolored). The colors stay on the
+ * device for phases with ordering 1 or 2. */
+vg_status vg_color(vg_ctx *ctx, vg_graph *g, int64_t n_hash, int32_t target_percent,
+                   int32_t single_iteration, int64_t *colors_out, int64_t *num_colors_out);
+/* Provide a coloring computed elsewhere (the ColorVector argument of the
+ * ...WithColoring / ...VertexOrder overloads); num_colors is the reference's
+ * numColor - 1. */
+vg_status vg_set_colors(vg_ctx *ctx, vg_graph *g, const int64_t *colors, int64_t num_colors);
+
+/* distbuildNextLevelGraph (rebuild.cpp:480-504) for one rank: replace g by the
+ * next-level graph. cvect NULL uses the communities of the last phase on g. */
+vg_status vg_rebuild(vg_ctx *ctx, vg_graph *g, const int64_t *cvect);
+
+/* The phase loop of graphClustering (main.cpp:242-513) run on the device:
+ * coloring at phase 0, phases, rebuilds, threshold cycling and the phase caps.
+ * g is not modified. levels receives up to max_levels entries; comm_out (may
+ * be NULL) receives the final community of every vertex of g, renumbered by
+ * sorted id exactly like graphClustering's -o output (main.cpp:381-425). */
+vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g, const vg_run_params *p,
+                         vg_level_stat *levels, int32_t max_levels, int32_t *nlevels_out,
+                         int64_t *comm_out);
+
+/* --- generators --------------------------------------------------------------- */
+
+/* generateInMemGraph for one rank (distgraph.cpp:391-407, 412-983): n points
+ * from Vite's LCG (seed 1), edge when the distance is at most r(n), weight =
+ * distance; bit-identical to the reference. extra_percent > 0 adds that
+ * percent of extra edges with U(0,1) weights drawn from `seed` (the
+ * reference's own extra edges are time-seeded, distgraph.cpp:755). */
+vg_status vg_generate_rgg(vg_ctx *ctx, int64_t n, double extra_percent, uint64_t seed,
+                          vg_graph **out);
+/* Seeded Barabasi-Albert (m attachments per vertex) and Erdos-Renyi G(n, M)
+ * graphs with unit weights, for the workloads the reference feeds through
+ * NetworKit (generators/nkit-ba.cpp:66-116, nkit-er.cpp:67); own designs. */
+vg_status vg_generate_ba(vg_ctx *ctx, int64_t n, int64_t m, uint64_t seed, vg_graph **out);
+vg_status vg_generate_er(vg_ctx *ctx, int64_t n, double avg_degree, uint64_t seed,
+                         vg_graph **out);
+/* Re-weight every edge: mode 1 = 1.0 (SET_EDGE_WEIGHTS_TO_ONE,
+ * distgraph.cpp:249-252), mode 2 = U(0,1) drawn per unordered pair from seed. */
+vg_status vg_graph_reweight(vg_ctx *ctx, vg_graph *g, int32_t mode, uint64_t seed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -324,3 +324,113 @@ def run_harness(args: list[str], record: str, threads: int = 1, timeout: float =
     res = subprocess.run([HARNESS, *args, "-w", record], capture_output=True, text=True,
                          env=env, timeout=timeout, check=True)
     return res.stdout
+
+
+@dataclass
+class LevelResult:
+    nv: int
+    ne: int
+    iters: int
+    mod: float
+    num_colors: int
+    cvect: np.ndarray
+    graph: Graph
+
+
+def run_levels(g: Graph, threshold: float = 1e-6, coloring: bool = False,
+               vertex_order: bool = False, max_colors: int = 8, single_color_iter: bool = False,
+               et_type: int = 0, et_delta: float = 1.0, threshold_scaling: bool = False,
+               one_phase: bool = False):
+    """The reference's phase loop (main.cpp:242-513) over the restatement, keeping every
+    level's graph and community vector. Returns (levels, colors of phase 0 or None)."""
+    levels = []
+    colors0 = None
+    cur = g
+    currMod, prevMod = -1.0, -1.0
+    phase = short_phase = tot_iters = 0
+    while True:
+        if threshold_scaling and not one_phase:
+            if short_phase > 12:
+                short_phase = 0
+            thr = (1e-3 if short_phase <= 2 else 1e-4 if short_phase <= 6
+                   else 1e-5 if short_phase <= 9 else threshold)
+        else:
+            thr = threshold
+        ncol = 0
+        if (coloring or vertex_order) and phase == 0:
+            colors0, ncol = color(cur, max_colors // 2, 70, single_color_iter)
+            cv, currMod, iters = louvain_phase(cur, thr, currMod, et_type, et_delta,
+                                               1 if coloring else 2, colors0, ncol + 1)
+        else:
+            cv, currMod, iters = louvain_phase(cur, thr, currMod, et_type, et_delta)
+        tot_iters += iters
+        levels.append(LevelResult(cur.nv, cur.ne, iters, currMod, ncol, cv, cur))
+        if currMod - prevMod > thr:
+            if not one_phase:
+                cur = rebuild(cur, cv)
+        else:
+            if threshold_scaling and not one_phase and phase < 10:
+                cv, currMod, iters = louvain_phase(cur, 1e-6, currMod)
+                levels.append(LevelResult(cur.nv, cur.ne, iters, currMod, 0, cv, cur))
+            break
+        prevMod, currMod = currMod, -1.0
+        phase += 1
+        if one_phase:
+            break
+        if threshold_scaling and not one_phase:
+            short_phase += 1
+        if phase == 200 or tot_iters > 10000:
+            break
+    return levels, colors0
+
+
+def flags_to_kwargs(flags: list[str]) -> dict:
+    """graphClustering flags (main.cpp:609-708) -> keyword arguments of run/run_levels."""
+    kw: dict = {}
+    i = 0
+    while i < len(flags):
+        f = flags[i]
+        if f in ("-c", "-d"):
+            parts = flags[i + 1].split(" ")
+            kw["max_colors"] = int(parts[0])
+            if len(parts) > 1:
+                kw["single_color_iter"] = parts[1].lower() in ("true", "1")
+            kw["coloring" if f == "-c" else "vertex_order"] = True
+            i += 2
+        elif f == "-t":
+            kw["et_type"] = int(flags[i + 1])
+            i += 2
+        elif f == "-a":
+            kw["et_delta"] = float(flags[i + 1])
+            i += 2
+        elif f == "-h":
+            kw["threshold"] = float(flags[i + 1])
+            i += 2
+        elif f == "-i":
+            kw["threshold_scaling"] = True
+            i += 1
+        elif f == "-p":
+            kw["one_phase"] = True
+            i += 1
+        else:
+            raise ValueError(f"unsupported flag {f}")
+    return kw
+
+
+def golden_graph(entry: dict) -> Graph:
+    """Rebuild the input graph of a golden case with the restatement's generators."""
+    src = entry["source"]
+    if src["kind"] == "reference_rgg":
+        return rgg(int(src["n"]))
+    kind, *rest = src["spec"].split(":")
+    if kind == "file":
+        base = {"rgg4k": 4096, "rgg64k": 65536}[rest[0]]
+        g = rgg(base)
+        return g.unit() if len(rest) > 1 and rest[1] == "unit" else g
+    if kind == "ba":
+        return ba(int(rest[0]), int(rest[1]), int(rest[2]))
+    if kind == "er":
+        return er(int(rest[0]), float(rest[1]), int(rest[2]))
+    if kind == "rggx":
+        return add_random_edges(rgg(int(rest[0])), float(rest[1]), int(rest[2]))[0]
+    raise ValueError(src)

@@ -1,0 +1,358 @@
+"""vite_b200: B200-native Louvain community detection (Vite's method) on one GPU.
+
+Python view of the C ABI in include/vite_b200.h (libvite_b200.so, built in this
+directory by ``make -C vite_b200/csrc``). The names follow the reference's
+operators: ``louvain_phase`` is distLouvainMethod and its variants,
+``color`` distColoringMultiHashMinMax, ``rebuild`` distbuildNextLevelGraph,
+``generate_rgg`` generateInMemGraph, ``run`` the phase loop of graphClustering.
+
+Importing this module loads the CUDA library; it raises if the library is
+missing, and every call runs on the GPU (there is no CPU path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvite_b200.so")
+HOST_LIB_PATH = os.path.join(HERE, "libvite_host.so")
+CLI_PATH = os.path.join(HERE, "graphClustering")
+
+EDGE_DTYPE = np.dtype([("tail", "<i8"), ("weight", "<f8")])
+
+VG_OK, VG_ERR_ARG, VG_ERR_OOM, VG_ERR_CUDA, VG_ERR_TIMEOUT, VG_ERR_STATE = range(6)
+_STATUS_NAMES = {0: "VG_OK", 1: "VG_ERR_ARG", 2: "VG_ERR_OOM", 3: "VG_ERR_CUDA",
+                 4: "VG_ERR_TIMEOUT", 5: "VG_ERR_STATE"}
+
+EXPORTED_SYMBOLS = [
+    "vg_ctx_create", "vg_ctx_destroy", "vg_last_error", "vg_ctx_bytes_in_use", "vg_ctx_profile",
+    "vg_ctx_stream",
+    "vg_graph_upload", "vg_graph_info", "vg_graph_download", "vg_graph_free", "vg_vertex_degree",
+    "vg_louvain_phase", "vg_color", "vg_set_colors", "vg_rebuild", "vg_louvain_run",
+    "vg_generate_rgg", "vg_generate_ba", "vg_generate_er", "vg_graph_reweight",
+]
+
+
+class VgError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class PhaseParams(C.Structure):
+    _fields_ = [("lower", C.c_double), ("threshold", C.c_double), ("et_type", C.c_int32),
+                ("et_delta", C.c_double), ("ordering", C.c_int32)]
+
+
+class RunParams(C.Structure):
+    _fields_ = [("threshold", C.c_double), ("coloring", C.c_int32), ("vertex_order", C.c_int32),
+                ("max_colors", C.c_int32), ("single_color_iter", C.c_int32),
+                ("et_type", C.c_int32), ("et_delta", C.c_double),
+                ("threshold_scaling", C.c_int32), ("one_phase", C.c_int32)]
+
+
+class LevelStat(C.Structure):
+    _fields_ = [("nv", C.c_int64), ("ne", C.c_int64), ("iters", C.c_int32),
+                ("modularity", C.c_double), ("num_colors", C.c_int64),
+                ("seconds_color", C.c_double), ("seconds_phase", C.c_double),
+                ("seconds_sweep", C.c_double), ("seconds_rebuild", C.c_double),
+                ("edges_swept", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_i64p = C.POINTER(C.c_int64)
+_f64p = C.POINTER(C.c_double)
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    """Load libvite_b200.so; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C vite_b200/csrc` "
+                              "(or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.vg_ctx_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(vp)]
+        L.vg_ctx_destroy.argtypes = [vp]
+        L.vg_last_error.argtypes = [vp]
+        L.vg_last_error.restype = C.c_char_p
+        L.vg_ctx_bytes_in_use.argtypes = [vp]
+        L.vg_ctx_bytes_in_use.restype = C.c_size_t
+        L.vg_ctx_profile.argtypes = [vp, C.c_int32, _f64p, _i64p, C.c_int32]
+        L.vg_ctx_stream.argtypes = [vp, C.POINTER(vp)]
+        L.vg_graph_upload.argtypes = [vp, C.c_int64, C.c_int64, _i64p, vp, C.POINTER(vp)]
+        L.vg_graph_info.argtypes = [vp, _i64p, _i64p]
+        L.vg_graph_download.argtypes = [vp, vp, _i64p, vp]
+        L.vg_graph_free.argtypes = [vp, vp]
+        L.vg_vertex_degree.argtypes = [vp, vp, _f64p, _f64p]
+        L.vg_louvain_phase.argtypes = [vp, vp, C.POINTER(PhaseParams), _i64p, _f64p,
+                                       C.POINTER(C.c_int32)]
+        L.vg_color.argtypes = [vp, vp, C.c_int64, C.c_int32, C.c_int32, _i64p, _i64p]
+        L.vg_set_colors.argtypes = [vp, vp, _i64p, C.c_int64]
+        L.vg_rebuild.argtypes = [vp, vp, _i64p]
+        L.vg_louvain_run.argtypes = [vp, vp, C.POINTER(RunParams), C.POINTER(LevelStat),
+                                     C.c_int32, C.POINTER(C.c_int32), _i64p]
+        L.vg_generate_rgg.argtypes = [vp, C.c_int64, C.c_double, C.c_uint64, C.POINTER(vp)]
+        L.vg_generate_ba.argtypes = [vp, C.c_int64, C.c_int64, C.c_uint64, C.POINTER(vp)]
+        L.vg_generate_er.argtypes = [vp, C.c_int64, C.c_double, C.c_uint64, C.POINTER(vp)]
+        L.vg_graph_reweight.argtypes = [vp, vp, C.c_int32, C.c_uint64]
+        for name in EXPORTED_SYMBOLS:
+            if name not in ("vg_last_error", "vg_ctx_bytes_in_use"):
+                getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray | None, ty=_i64p):
+    return None if a is None else a.ctypes.data_as(ty)
+
+
+@dataclass
+class Levels:
+    stats: list
+    comm: np.ndarray | None
+
+
+class Graph:
+    """A CSR resident on the device (vg_graph)."""
+
+    def __init__(self, ctx: "Context", handle: C.c_void_p):
+        self.ctx = ctx
+        self.handle = handle
+
+    @property
+    def nv(self) -> int:
+        nv = C.c_int64()
+        lib().vg_graph_info(self.handle, C.byref(nv), None)
+        return nv.value
+
+    @property
+    def ne(self) -> int:
+        ne = C.c_int64()
+        lib().vg_graph_info(self.handle, None, C.byref(ne))
+        return ne.value
+
+    def download(self):
+        """(rowptr int64[nv+1], tail int64[ne], weight float64[ne]) in Vite's layout."""
+        nv, ne = self.nv, self.ne
+        rp = np.empty(nv + 1, np.int64)
+        edges = np.empty(ne, EDGE_DTYPE)
+        self.ctx._check(lib().vg_graph_download(self.ctx.handle, self.handle, _ptr(rp),
+                                                edges.ctypes.data if ne else None))
+        return rp, edges["tail"].copy(), edges["weight"].copy()
+
+    def free(self):
+        if self.handle:
+            self.ctx._check(lib().vg_graph_free(self.ctx.handle, self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            if self.handle and self.ctx.handle:
+                lib().vg_graph_free(self.ctx.handle, self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class Context:
+    """vg_ctx: one device, one stream, an optional device-memory budget."""
+
+    def __init__(self, device: int = 0, mem_budget: int = 0):
+        h = C.c_void_p()
+        st = lib().vg_ctx_create(device, mem_budget, C.byref(h))
+        if st != VG_OK:
+            raise VgError(st, f"vg_ctx_create(device={device}) failed")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib().vg_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != VG_OK:
+            raise VgError(st, lib().vg_last_error(self.handle).decode())
+
+    @property
+    def bytes_in_use(self) -> int:
+        return int(lib().vg_ctx_bytes_in_use(self.handle))
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the context, as an integer handle."""
+        s = C.c_void_p()
+        self._check(lib().vg_ctx_stream(self.handle, C.byref(s)))
+        return s.value or 0
+
+    def profile(self, enable: bool, reset: bool = True) -> tuple[float, int]:
+        ms = C.c_double()
+        n = C.c_int64()
+        self._check(lib().vg_ctx_profile(self.handle, int(enable), C.byref(ms), C.byref(n),
+                                         int(reset)))
+        return ms.value, n.value
+
+    # graphs ---------------------------------------------------------------------------
+    def upload(self, rowptr, tail, weight) -> Graph:
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+        nv = len(rowptr) - 1
+        ne = len(tail)
+        edges = np.empty(ne, EDGE_DTYPE)
+        edges["tail"] = tail
+        edges["weight"] = weight
+        h = C.c_void_p()
+        self._check(lib().vg_graph_upload(self.handle, nv, ne, _ptr(rowptr),
+                                          edges.ctypes.data if ne else None, C.byref(h)))
+        return Graph(self, h)
+
+    def upload_edges(self, rowptr: np.ndarray, edges: np.ndarray) -> Graph:
+        """Upload from a Vite Edge array (structured int64 tail / float64 weight)."""
+        h = C.c_void_p()
+        self._check(lib().vg_graph_upload(self.handle, len(rowptr) - 1, len(edges), _ptr(rowptr),
+                                          edges.ctypes.data if len(edges) else None, C.byref(h)))
+        return Graph(self, h)
+
+    def generate_rgg(self, n: int, extra_percent: float = 0.0, seed: int = 0) -> Graph:
+        h = C.c_void_p()
+        self._check(lib().vg_generate_rgg(self.handle, n, extra_percent, seed, C.byref(h)))
+        return Graph(self, h)
+
+    def generate_ba(self, n: int, m: int, seed: int) -> Graph:
+        h = C.c_void_p()
+        self._check(lib().vg_generate_ba(self.handle, n, m, seed, C.byref(h)))
+        return Graph(self, h)
+
+    def generate_er(self, n: int, avg_degree: float, seed: int) -> Graph:
+        h = C.c_void_p()
+        self._check(lib().vg_generate_er(self.handle, n, avg_degree, seed, C.byref(h)))
+        return Graph(self, h)
+
+    def reweight(self, g: Graph, mode: int, seed: int = 0) -> None:
+        self._check(lib().vg_graph_reweight(self.handle, g.handle, mode, seed))
+
+    # the Louvain path ---------------------------------------------------------------
+    def vertex_degree(self, g: Graph):
+        vd = np.empty(g.nv, np.float64)
+        c = C.c_double()
+        self._check(lib().vg_vertex_degree(self.handle, g.handle, _ptr(vd, _f64p), C.byref(c)))
+        return vd, c.value
+
+    def louvain_phase(self, g: Graph, threshold: float = 1e-6, lower: float = -1.0,
+                      et_type: int = 0, et_delta: float = 1.0, ordering: int = 0,
+                      want_cvect: bool = True):
+        p = PhaseParams(lower, threshold, et_type, et_delta, ordering)
+        cv = np.empty(g.nv, np.int64) if want_cvect else None
+        mod = C.c_double()
+        it = C.c_int32()
+        self._check(lib().vg_louvain_phase(self.handle, g.handle, C.byref(p), _ptr(cv),
+                                           C.byref(mod), C.byref(it)))
+        return cv, mod.value, it.value
+
+    def color(self, g: Graph, n_hash: int, target_percent: int = 70, single: bool = False):
+        out = np.empty(g.nv, np.int64)
+        nc = C.c_int64()
+        self._check(lib().vg_color(self.handle, g.handle, n_hash, target_percent, int(single),
+                                   _ptr(out), C.byref(nc)))
+        return out, nc.value
+
+    def set_colors(self, g: Graph, colors: np.ndarray, num_colors: int) -> None:
+        colors = np.ascontiguousarray(colors, dtype=np.int64)
+        self._check(lib().vg_set_colors(self.handle, g.handle, _ptr(colors), num_colors))
+
+    def rebuild(self, g: Graph, cvect: np.ndarray | None = None) -> None:
+        cv = None if cvect is None else np.ascontiguousarray(cvect, dtype=np.int64)
+        self._check(lib().vg_rebuild(self.handle, g.handle, _ptr(cv)))
+
+    def run(self, g: Graph, threshold: float = 1e-6, coloring: bool = False,
+            vertex_order: bool = False, max_colors: int = 8, single_color_iter: bool = False,
+            et_type: int = 0, et_delta: float = 1.0, threshold_scaling: bool = False,
+            one_phase: bool = False, want_comm: bool = False, max_levels: int = 256) -> Levels:
+        p = RunParams(threshold, int(coloring), int(vertex_order), max_colors,
+                      int(single_color_iter), et_type, et_delta, int(threshold_scaling),
+                      int(one_phase))
+        stats = (LevelStat * max_levels)()
+        n = C.c_int32()
+        comm = np.empty(g.nv, np.int64) if want_comm else None
+        self._check(lib().vg_louvain_run(self.handle, g.handle, C.byref(p), stats, max_levels,
+                                         C.byref(n), _ptr(comm)))
+        return Levels([stats[i].as_dict() for i in range(min(n.value, max_levels))], comm)
+
+
+@dataclass
+class LevelOut:
+    nv: int
+    ne: int
+    iters: int
+    mod: float
+    num_colors: int
+    cvect: np.ndarray
+
+
+def run_levels(ctx: Context, g: Graph, threshold: float = 1e-6, coloring: bool = False,
+               vertex_order: bool = False, max_colors: int = 8, single_color_iter: bool = False,
+               et_type: int = 0, et_delta: float = 1.0, threshold_scaling: bool = False,
+               one_phase: bool = False) -> list[LevelOut]:
+    """graphClustering's phase loop (main.cpp:242-513) driven from the host through the
+    per-operator entry points, returning every level's community vector. The graph g is
+    coarsened in place, as distbuildNextLevelGraph replaces the DistGraph it is given."""
+    out: list[LevelOut] = []
+    currMod, prevMod = -1.0, -1.0
+    phase = short_phase = tot_iters = 0
+    while True:
+        if threshold_scaling and not one_phase:
+            if short_phase > 12:
+                short_phase = 0
+            thr = (1e-3 if short_phase <= 2 else 1e-4 if short_phase <= 6
+                   else 1e-5 if short_phase <= 9 else threshold)
+        else:
+            thr = threshold
+        ncol = 0
+        ordering = 0
+        if (coloring or vertex_order) and phase == 0:
+            _, ncol = ctx.color(g, max_colors // 2, 70, single_color_iter)
+            ordering = 1 if coloring else 2
+        nv, ne = g.nv, g.ne
+        cv, currMod, iters = ctx.louvain_phase(g, thr, currMod, et_type, et_delta, ordering)
+        tot_iters += iters
+        out.append(LevelOut(nv, ne, iters, currMod, ncol, cv))
+        if currMod - prevMod > thr:
+            if not one_phase:
+                ctx.rebuild(g)
+        else:
+            if threshold_scaling and not one_phase and phase < 10:
+                cv, currMod, iters = ctx.louvain_phase(g, 1e-6, currMod)
+                out.append(LevelOut(g.nv, g.ne, iters, currMod, 0, cv))
+            break
+        prevMod, currMod = currMod, -1.0
+        phase += 1
+        if one_phase:
+            break
+        if threshold_scaling and not one_phase:
+            short_phase += 1
+        if phase == 200 or tot_iters > 10000:
+            break
+    return out

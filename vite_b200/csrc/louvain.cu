@@ -1,0 +1,1075 @@
+// One Louvain phase on the device: distLouvainMethod and its early-termination,
+// coloring and vertex-ordering variants (louvain.cpp:7-1938), for one rank.
+//
+// Per iteration:
+//   sweep      distExecuteLouvainIteration + distBuildLocalMapCounter +
+//              distGetMaxIndex (louvain.cpp:2220-2466), one kernel per degree class
+//              over precomputed vertex lists; moves go to FP64/int delta arrays
+//              with atomics (the localCupdate of louvain.cpp:2351-2410);
+//   apply+mod  distUpdateLocalCinfo + distComputeModularity (louvain.cpp:2468-2547)
+//              fused: deltas folded into the community info while the two sums
+//              of the modularity are reduced deterministically;
+//   swap       pointer rotation (plain) or the early-termination swaps.
+// Arithmetic follows the reference's expression order with explicit
+// round-to-nearest intrinsics, so no multiply-add is ever fused.
+#include "vg_internal.cuh"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+
+namespace {
+
+constexpr int NCLS = 7;
+// class by degree: 0:<=4 1:<=8 2:<=16 3:<=32 (sub-warp groups, one chunk)
+// 4:<=WT_MAXDEG (warp, shared-memory table) 5:<=CT_MAXDEG (CTA, shared table)
+// 6: above (CTA, table in global scratch)
+constexpr int WT_MAXDEG = 512;
+constexpr int WT_CAP = 1024;
+constexpr int WT_WARPS = 4;
+constexpr int CT_MAXDEG = 4096;
+constexpr int CT_CAP = 8192;
+constexpr int CT_THREADS = 256;
+constexpr int32_t EMPTY = -1;
+
+__host__ __device__ __forceinline__ int degree_class(int64_t d) {
+    if (d <= 4) return 0;
+    if (d <= 8) return 1;
+    if (d <= 16) return 2;
+    if (d <= 32) return 3;
+    if (d <= WT_MAXDEG) return 4;
+    if (d <= CT_MAXDEG) return 5;
+    return 6;
+}
+
+struct SweepArgs {
+    const int64_t *__restrict__ rowptr;
+    const int32_t *__restrict__ tail;
+    const double *__restrict__ weight;
+    const int32_t *__restrict__ curr;
+    int32_t *__restrict__ target;
+    const double *__restrict__ vdeg;
+    const double *__restrict__ cdeg;
+    const int32_t *__restrict__ csize;
+    double *__restrict__ udeg;
+    int32_t *__restrict__ usize;
+    double *__restrict__ cw;
+    double *__restrict__ frozen;
+    const uint8_t *__restrict__ active; // nullptr when early termination is off
+    double constant;
+};
+
+// gain of moving to a community (louvain.cpp:2263), evaluated in the reference's order
+__device__ __forceinline__ double gain_of(double eiy, double eix, double vd, double ay, double ax,
+                                          double constant) {
+    const double first = __dmul_rn(2.0, __dsub_rn(eiy, eix));
+    const double second = __dmul_rn(__dmul_rn(__dmul_rn(2.0, vd), __dsub_rn(ay, ax)), constant);
+    return __dsub_rn(first, second);
+}
+
+// (gain, id) ordering of distGetMaxIndex: larger gain wins, equal gains go to the smaller id
+__device__ __forceinline__ bool better(bool ok_a, double g_a, int32_t c_a, bool ok_b, double g_b,
+                                       int32_t c_b) {
+    if (!ok_a) return false;
+    if (!ok_b) return true;
+    return g_a > g_b || (g_a == g_b && c_a < c_b);
+}
+
+// decision + bookkeeping shared by all kernels (louvain.cpp:2275-2416)
+__device__ __forceinline__ void commit_vertex(const SweepArgs &a, int32_t v, int32_t cc,
+                                              int32_t ccSize, double vd, bool has_edges,
+                                              double counter0, bool ok, int32_t cand, int32_t csz) {
+    int32_t tgt = cc;
+    if (has_edges) {
+        int32_t maxSize = ccSize;
+        if (ok) {
+            tgt = cand;
+            maxSize = csz;
+        }
+        if (maxSize == 1 && ccSize == 1 && tgt > cc) tgt = cc;
+    }
+    const double cwv = has_edges ? counter0 : 0.0;
+    a.cw[v] = cwv;
+    if (a.active) a.frozen[v] = cwv;
+    a.target[v] = tgt;
+    if (tgt != cc) {
+        atomicAdd(&a.udeg[tgt], vd);
+        atomicAdd(&a.usize[tgt], 1);
+        atomicAdd(&a.udeg[cc], -vd);
+        atomicAdd(&a.usize[cc], -1);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// classes 0-3: G lanes per vertex, all edges in one chunk (degree <= G)
+
+template <int G>
+__global__ void __launch_bounds__(256) k_sweep_group(SweepArgs a, const int32_t *__restrict__ list,
+                                                     int64_t count) {
+    __shared__ double stage[256];
+    constexpr int GPW = 32 / G;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & (G - 1);
+    const int grp = lane / G;
+    const unsigned gmask = (G == 32) ? full : (((1u << G) - 1u) << (grp * G));
+    double *my = stage + (threadIdx.x & ~31);
+    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = wg * GPW; base < count; base += nw * GPW) {
+        const int64_t idx = base + grp;
+        int32_t v = 0, cc = 0;
+        int64_t e0 = 0;
+        int d = 0;
+        bool run = false;
+        if (idx < count) {
+            v = list[idx];
+            e0 = a.rowptr[v];
+            d = (int)(a.rowptr[v + 1] - e0);
+            cc = a.curr[v];
+            run = true;
+            if (a.active && !a.active[v]) {
+                run = false;
+                if (sub == 0) a.cw[v] = a.frozen[v];
+            }
+        }
+        const bool has = run && sub < d;
+        int32_t t = -1, c = -1;
+        double w = 0.0;
+        if (has) {
+            t = a.tail[e0 + sub];
+            w = a.weight[e0 + sub];
+            c = a.curr[t];
+        }
+        my[lane] = w;
+        const uint64_t key = has ? (((uint64_t)grp << 32) | (uint32_t)c)
+                                 : (0xFFFFFFFF00000000ULL | (uint64_t)lane);
+        const unsigned peers = __match_any_sync(full, key);
+        __syncwarp();
+        const int leader = __ffs(peers) - 1;
+        double sum = 0.0;
+        if (has && lane == leader) {
+            // counter of this community: weights folded in CSR order
+            unsigned m = peers & (peers - 1);
+            sum = my[leader];
+            while (m) {
+                const int b = __ffs(m) - 1;
+                sum = __dadd_rn(sum, my[b]);
+                m &= m - 1;
+            }
+        }
+        const unsigned selfm = __ballot_sync(full, has && t == v) & gmask;
+        double selfLoop = 0.0;
+        {
+            unsigned m = selfm;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                selfLoop = __dadd_rn(selfLoop, my[b]);
+                m &= m - 1;
+            }
+        }
+        const unsigned ccm = __ballot_sync(full, has && c == cc) & gmask;
+        const double cnt0 = __shfl_sync(full, sum, ccm ? (__ffs(ccm) - 1) : lane);
+        const double counter0 = ccm ? cnt0 : 0.0;
+        double vd = 0.0, ccDeg = 0.0;
+        int32_t ccSize = 0;
+        if (run) {
+            vd = a.vdeg[v];
+            ccDeg = a.cdeg[cc];
+            ccSize = a.csize[cc];
+        }
+        double gain = 0.0;
+        int32_t cand = INT_MAX, csz = 0;
+        bool ok = false;
+        if (has && lane == leader && c != cc) {
+            const double ay = a.cdeg[c];
+            csz = a.csize[c];
+            gain = gain_of(sum, __dsub_rn(counter0, selfLoop), vd, ay, __dsub_rn(ccDeg, vd),
+                           a.constant);
+            ok = gain > 0.0;
+            cand = c;
+        }
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) {
+            const double og = __shfl_xor_sync(full, gain, o);
+            const int32_t oc = __shfl_xor_sync(full, cand, o);
+            const int32_t os = __shfl_xor_sync(full, csz, o);
+            const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
+            if (better(ook, og, oc, ok, gain, cand)) {
+                gain = og;
+                cand = oc;
+                csz = os;
+                ok = true;
+            }
+        }
+        if (run && sub == 0) commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, cand, csz);
+        __syncwarp();
+    }
+}
+
+// open addressing: multiplicative hash, linear probing
+__device__ __forceinline__ uint32_t slot_hash(int32_t c, int logcap) {
+    return ((uint32_t)c * 2654435761u) >> (32 - logcap);
+}
+
+// ---------------------------------------------------------------------------------
+// class 4: one warp per vertex, table in shared memory private to the warp.
+// Chunks of 32 edges; inside a chunk one leader per community folds its lanes'
+// weights in CSR order onto the table value, so each counter is the reference's
+// exact left fold.
+
+__global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
+                                                               const int32_t *__restrict__ list,
+                                                               int64_t count) {
+    extern __shared__ unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *vals = reinterpret_cast<double *>(smem_raw) + (size_t)warp * WT_CAP;
+    int32_t *keys = reinterpret_cast<int32_t *>(reinterpret_cast<double *>(smem_raw) +
+                                                (size_t)WT_WARPS * WT_CAP) +
+                    (size_t)warp * WT_CAP;
+    double *stage = reinterpret_cast<double *>(reinterpret_cast<int32_t *>(
+                        reinterpret_cast<double *>(smem_raw) + (size_t)WT_WARPS * WT_CAP) +
+                                               (size_t)WT_WARPS * WT_CAP) +
+                    (size_t)warp * 32;
+    const unsigned full = 0xffffffffu;
+    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t idx = wg; idx < count; idx += nw) {
+        const int32_t v = list[idx];
+        const int32_t cc = a.curr[v];
+        if (a.active && !a.active[v]) {
+            if (lane == 0) a.cw[v] = a.frozen[v];
+            continue;
+        }
+        const int64_t e0 = a.rowptr[v];
+        const int d = (int)(a.rowptr[v + 1] - e0);
+        int logcap = 5;
+        while ((1 << logcap) < 2 * d) logcap++;
+        const int cap = 1 << logcap;
+        for (int s = lane; s < cap; s += 32) keys[s] = EMPTY;
+        __syncwarp();
+        double selfLoop = 0.0;
+        for (int off = 0; off < d; off += 32) {
+            const int k = off + lane;
+            const bool has = k < d;
+            int32_t t = -1, c = -1;
+            double w = 0.0;
+            if (has) {
+                t = a.tail[e0 + k];
+                w = a.weight[e0 + k];
+                c = a.curr[t];
+            }
+            stage[lane] = w;
+            const unsigned peers = __match_any_sync(full, has ? c : (-1 - lane));
+            __syncwarp();
+            if (has && lane == __ffs(peers) - 1) {
+                uint32_t h = slot_hash(c, logcap);
+                bool fresh = false;
+                for (;;) {
+                    const int32_t kk = keys[h];
+                    if (kk == c) break;
+                    if (kk == EMPTY) {
+                        const int32_t old = atomicCAS(&keys[h], EMPTY, c);
+                        if (old == EMPTY) {
+                            fresh = true;
+                            break;
+                        }
+                        if (old == c) break;
+                    }
+                    h = (h + 1) & (cap - 1);
+                }
+                unsigned m = peers & (peers - 1);
+                double acc = fresh ? stage[lane] : __dadd_rn(vals[h], stage[lane]);
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    acc = __dadd_rn(acc, stage[b]);
+                    m &= m - 1;
+                }
+                vals[h] = acc;
+            }
+            const unsigned selfm = __ballot_sync(full, has && t == v);
+            {
+                unsigned m = selfm;
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    selfLoop = __dadd_rn(selfLoop, stage[b]);
+                    m &= m - 1;
+                }
+            }
+            __syncwarp();
+        }
+        // counter[0]: the current community's entry, if any neighbour is in it
+        double counter0 = 0.0;
+        {
+            uint32_t h = slot_hash(cc, logcap);
+            for (int probe = 0; probe < cap; probe++) {
+                const int32_t kk = keys[h];
+                if (kk == cc) {
+                    counter0 = vals[h];
+                    break;
+                }
+                if (kk == EMPTY) break;
+                h = (h + 1) & (cap - 1);
+            }
+        }
+        const double vd = a.vdeg[v];
+        const double ccDeg = a.cdeg[cc];
+        const int32_t ccSize = a.csize[cc];
+        const double eix = __dsub_rn(counter0, selfLoop);
+        const double ax = __dsub_rn(ccDeg, vd);
+        double gain = 0.0;
+        int32_t cand = INT_MAX, csz = 0;
+        bool ok = false;
+        for (int s = lane; s < cap; s += 32) {
+            const int32_t kk = keys[s];
+            if (kk == EMPTY || kk == cc) continue;
+            const double g = gain_of(vals[s], eix, vd, a.cdeg[kk], ax, a.constant);
+            if (g > 0.0 && better(true, g, kk, ok, gain, cand)) {
+                gain = g;
+                cand = kk;
+                csz = a.csize[kk];
+                ok = true;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double og = __shfl_xor_sync(full, gain, o);
+            const int32_t oc = __shfl_xor_sync(full, cand, o);
+            const int32_t os = __shfl_xor_sync(full, csz, o);
+            const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
+            if (better(ook, og, oc, ok, gain, cand)) {
+                gain = og;
+                cand = oc;
+                csz = os;
+                ok = true;
+            }
+        }
+        if (lane == 0) commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, cand, csz);
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// classes 5-6: one CTA per vertex. Warps take 32-edge slices of each 256-edge
+// chunk; inside a slice the leader folds its lanes in CSR order, and the slices
+// meet in the table through atomics (table in shared memory, or in a global
+// scratch region per CTA for the largest degrees).
+
+struct CtaShared {
+    double red_g[CT_THREADS / 32];
+    int32_t red_c[CT_THREADS / 32];
+    int32_t red_s[CT_THREADS / 32];
+    int red_ok[CT_THREADS / 32];
+    double self_part[CT_THREADS / 32];
+    double counter0;
+};
+
+template <bool GLOBAL_TABLE>
+__global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int32_t *__restrict__ list,
+                                                          int64_t count, int32_t *__restrict__ gkeys,
+                                                          double *__restrict__ gvals, int64_t gcap) {
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ CtaShared sh;
+    __shared__ double stage[CT_THREADS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    double *vals;
+    int32_t *keys;
+    if (GLOBAL_TABLE) {
+        vals = gvals + (size_t)blockIdx.x * gcap;
+        keys = gkeys + (size_t)blockIdx.x * gcap;
+    } else {
+        vals = reinterpret_cast<double *>(smem_raw);
+        keys = reinterpret_cast<int32_t *>(vals + CT_CAP);
+    }
+    for (int64_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+        const int32_t v = list[idx];
+        const int32_t cc = a.curr[v];
+        if (a.active && !a.active[v]) {
+            if (threadIdx.x == 0) a.cw[v] = a.frozen[v];
+            continue;
+        }
+        const int64_t e0 = a.rowptr[v];
+        const int64_t d = a.rowptr[v + 1] - e0;
+        int logcap = 5;
+        while (((int64_t)1 << logcap) < 2 * d) logcap++;
+        const int64_t cap = (int64_t)1 << logcap;
+        for (int64_t s = threadIdx.x; s < cap; s += CT_THREADS) {
+            keys[s] = EMPTY;
+            vals[s] = 0.0;
+        }
+        double selfLoop = 0.0; // per-warp partial, in CSR order inside the warp's slices
+        __syncthreads();
+        for (int64_t off = 0; off < d; off += CT_THREADS) {
+            const int64_t k = off + threadIdx.x;
+            const bool has = k < d;
+            int32_t t = -1, c = -1;
+            double w = 0.0;
+            if (has) {
+                t = a.tail[e0 + k];
+                w = a.weight[e0 + k];
+                c = a.curr[t];
+            }
+            stage[threadIdx.x] = w;
+            const unsigned peers = __match_any_sync(full, has ? c : (-1 - lane));
+            __syncwarp();
+            if (has && lane == __ffs(peers) - 1) {
+                double acc = stage[threadIdx.x];
+                unsigned m = peers & (peers - 1);
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    acc = __dadd_rn(acc, stage[(threadIdx.x & ~31) + b]);
+                    m &= m - 1;
+                }
+                uint32_t h = slot_hash(c, logcap);
+                for (;;) {
+                    const int32_t kk = keys[h];
+                    if (kk == c) break;
+                    if (kk == EMPTY) {
+                        const int32_t old = atomicCAS(&keys[h], EMPTY, c);
+                        if (old == EMPTY || old == c) break;
+                    }
+                    h = (h + 1) & (uint32_t)(cap - 1);
+                }
+                atomicAdd(&vals[h], acc);
+            }
+            const unsigned selfm = __ballot_sync(full, has && t == v);
+            {
+                unsigned m = selfm;
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    selfLoop = __dadd_rn(selfLoop, stage[(threadIdx.x & ~31) + b]);
+                    m &= m - 1;
+                }
+            }
+            __syncwarp();
+        }
+        if (lane == 0) sh.self_part[warp] = selfLoop;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int w = 0; w < CT_THREADS / 32; w++) s = __dadd_rn(s, sh.self_part[w]);
+            sh.self_part[0] = s;
+            double c0 = 0.0;
+            uint32_t h = slot_hash(cc, logcap);
+            for (int64_t probe = 0; probe < cap; probe++) {
+                const int32_t kk = keys[h];
+                if (kk == cc) {
+                    c0 = vals[h];
+                    break;
+                }
+                if (kk == EMPTY) break;
+                h = (h + 1) & (uint32_t)(cap - 1);
+            }
+            sh.counter0 = c0;
+        }
+        __syncthreads();
+        const double counter0 = sh.counter0;
+        selfLoop = sh.self_part[0];
+        const double vd = a.vdeg[v];
+        const double ccDeg = a.cdeg[cc];
+        const int32_t ccSize = a.csize[cc];
+        const double eix = __dsub_rn(counter0, selfLoop);
+        const double ax = __dsub_rn(ccDeg, vd);
+        double gain = 0.0;
+        int32_t cand = INT_MAX, csz = 0;
+        bool ok = false;
+        for (int64_t s = threadIdx.x; s < cap; s += CT_THREADS) {
+            const int32_t kk = keys[s];
+            if (kk == EMPTY || kk == cc) continue;
+            const double g = gain_of(vals[s], eix, vd, a.cdeg[kk], ax, a.constant);
+            if (g > 0.0 && better(true, g, kk, ok, gain, cand)) {
+                gain = g;
+                cand = kk;
+                csz = a.csize[kk];
+                ok = true;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double og = __shfl_xor_sync(full, gain, o);
+            const int32_t oc = __shfl_xor_sync(full, cand, o);
+            const int32_t os = __shfl_xor_sync(full, csz, o);
+            const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
+            if (better(ook, og, oc, ok, gain, cand)) {
+                gain = og;
+                cand = oc;
+                csz = os;
+                ok = true;
+            }
+        }
+        if (lane == 0) {
+            sh.red_g[warp] = gain;
+            sh.red_c[warp] = cand;
+            sh.red_s[warp] = csz;
+            sh.red_ok[warp] = ok;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < CT_THREADS / 32; w++) {
+                if (better(sh.red_ok[w] != 0, sh.red_g[w], sh.red_c[w], ok, gain, cand)) {
+                    gain = sh.red_g[w];
+                    cand = sh.red_c[w];
+                    csz = sh.red_s[w];
+                    ok = true;
+                }
+            }
+            commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, cand, csz);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// init, degree, apply + modularity, swaps
+
+// distSumVertexDegree (louvain.cpp:2161-2186): each row summed in CSR order
+__global__ void k_degree(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
+                         int64_t nv, double *__restrict__ vdeg) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double tw = 0.0;
+        const int64_t e1 = rowptr[i + 1];
+        for (int64_t k = rowptr[i]; k < e1; k++) tw = __dadd_rn(tw, w[k]);
+        vdeg[i] = tw;
+    }
+}
+
+// distInitLouvain (louvain.cpp:2138-2159) plus the early-termination buffers
+__global__ void k_init(int64_t nv, const double *__restrict__ vdeg, double *__restrict__ cdeg,
+                       int32_t *__restrict__ csize, double *__restrict__ udeg,
+                       int32_t *__restrict__ usize, int32_t *__restrict__ past,
+                       int32_t *__restrict__ curr, int32_t *__restrict__ target,
+                       uint8_t *__restrict__ active, double *__restrict__ pcurr,
+                       double *__restrict__ pprev) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        cdeg[i] = vdeg[i];
+        csize[i] = 1;
+        udeg[i] = 0.0;
+        usize[i] = 0;
+        past[i] = (int32_t)i;
+        curr[i] = (int32_t)i;
+        target[i] = (int32_t)i;
+        if (active) active[i] = 1;
+        if (pcurr) pcurr[i] = 0.0; // value-initialised (louvain.cpp:244-249)
+        if (pprev) pprev[i] = 1.0;
+    }
+}
+
+__device__ double block_sum(double v, double *ws) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_down_sync(0xffffffffu, v, o));
+    if (lane == 0) ws[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (warp == 0) {
+        s = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s = __dadd_rn(s, __shfl_down_sync(0xffffffffu, s, o));
+    }
+    __syncthreads();
+    return s;
+}
+
+constexpr int APPLY_BLOCKS = 592; // 4 per SM on a 148-SM part; fixed so sums are reproducible
+constexpr int APPLY_THREADS = 512;
+
+// distUpdateLocalCinfo (louvain.cpp:2534-2547) fused with the two sums of
+// distComputeModularity (louvain.cpp:2496-2504) and the frozen-vertex count
+__global__ void __launch_bounds__(APPLY_THREADS) k_apply_mod(
+    int64_t nv, double *__restrict__ cdeg, int32_t *__restrict__ csize, double *__restrict__ udeg,
+    int32_t *__restrict__ usize, const double *__restrict__ cw, const uint8_t *__restrict__ active,
+    int do_sums, double *__restrict__ part) {
+    __shared__ double ws[32];
+    double le = 0.0, la2 = 0.0, frozen = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double du = udeg[i];
+        const int32_t ds = usize[i];
+        double cd = cdeg[i];
+        if (ds != 0 || du != 0.0) {
+            cd = __dadd_rn(cd, du);
+            cdeg[i] = cd;
+            csize[i] += ds;
+            udeg[i] = 0.0;
+            usize[i] = 0;
+        }
+        if (do_sums) {
+            le = __dadd_rn(le, cw[i]);
+            la2 = __dadd_rn(la2, __dmul_rn(cd, cd));
+            if (active && !active[i]) frozen += 1.0;
+        }
+    }
+    if (!do_sums) return;
+    le = block_sum(le, ws);
+    la2 = block_sum(la2, ws);
+    frozen = block_sum(frozen, ws);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x + 0] = le;
+        part[3 * blockIdx.x + 1] = la2;
+        part[3 * blockIdx.x + 2] = frozen;
+    }
+}
+
+// final reduction and the ABS_MOD_PER_ITER modularity (louvain.cpp:2518-2524)
+__global__ void k_mod_final(const double *__restrict__ part, int nblk, double constant,
+                            double *__restrict__ out) {
+    __shared__ double ws[32];
+    double le = 0.0, la2 = 0.0, fr = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+        le = __dadd_rn(le, part[3 * b]);
+        la2 = __dadd_rn(la2, part[3 * b + 1]);
+        fr += part[3 * b + 2];
+    }
+    le = block_sum(le, ws);
+    la2 = block_sum(la2, ws);
+    fr = block_sum(fr, ws);
+    if (threadIdx.x == 0) {
+        const double m = __dsub_rn(__dmul_rn(le, constant),
+                                   __dmul_rn(__dmul_rn(la2, constant), constant));
+        out[0] = fabs(m);
+        out[1] = fr;
+        out[2] = le;
+        out[3] = la2;
+    }
+}
+
+// early termination -t 1/3 (louvain.cpp:172-184): C++'s chained
+// `target == curr == past` compares the bool (target == curr) with past
+__global__ void k_swap_et13(int64_t nv, int numIters, int32_t *__restrict__ past,
+                            int32_t *__restrict__ curr, int32_t *__restrict__ target,
+                            uint8_t *__restrict__ active) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t p = past[i], c = curr[i], t = target[i];
+        if (numIters > 2 && ((int32_t)(t == c) == p)) {
+            active[i] = 0;
+        } else {
+            past[i] = c;
+            curr[i] = t;
+            target[i] = p;
+        }
+    }
+}
+
+// early termination -t 2/4 (louvain.cpp:381-400)
+__global__ void k_swap_et24(int64_t nv, int numIters, double one_minus_delta,
+                            int32_t *__restrict__ past, int32_t *__restrict__ curr,
+                            int32_t *__restrict__ target, uint8_t *__restrict__ active,
+                            double *__restrict__ pcurr, const double *__restrict__ pprev) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (!active[i]) continue;
+        const int32_t p = past[i], c = curr[i];
+        bool act = true;
+        if (numIters > 2 && c == p) {
+            const double pc = __dmul_rn(pprev[i], one_minus_delta);
+            pcurr[i] = pc;
+            if (pc <= 0.02) { // P_CUTOFF (louvain.hpp:74)
+                act = false;
+                active[i] = 0;
+            }
+        }
+        if (act) {
+            past[i] = c;
+            curr[i] = target[i];
+            target[i] = p;
+        }
+    }
+}
+
+__global__ void k_widen(const int32_t *__restrict__ in, int64_t n, int64_t *__restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[i];
+}
+
+__global__ void k_narrow(const int64_t *__restrict__ in, int64_t n, int64_t lim,
+                         int32_t *__restrict__ out, int *__restrict__ bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t x = in[i];
+        if (x < -1 || x >= lim) *bad = 1;
+        out[i] = (int32_t)x;
+    }
+}
+
+// bucket key of a vertex: (color bucket, degree class)
+__global__ void k_bucket_keys(const int64_t *__restrict__ rowptr, int64_t nv,
+                              const int32_t *__restrict__ colors, int64_t numColor,
+                              int32_t *__restrict__ key, int32_t *__restrict__ counts,
+                              unsigned long long *__restrict__ maxdeg) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = rowptr[i + 1] - rowptr[i];
+        int64_t cb = 0;
+        if (colors) cb = colors[i] < 0 ? numColor - 1 : colors[i];
+        const int32_t k = (int32_t)(cb * NCLS + degree_class(d));
+        key[i] = k;
+        atomicAdd(&counts[k], 1);
+        if (d > CT_MAXDEG) atomicMax(maxdeg, (unsigned long long)d);
+    }
+}
+
+__global__ void k_bucket_scatter(int64_t nv, const int32_t *__restrict__ key,
+                                 int32_t *__restrict__ fill, int32_t *__restrict__ list) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+         i += (int64_t)gridDim.x * blockDim.x)
+        list[atomicAdd(&fill[key[i]], 1)] = (int32_t)i;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------------
+// host side
+
+struct Buckets {
+    DevBuf<int32_t> list;
+    std::vector<int64_t> start; // (numColor * NCLS) + 1 offsets
+    int64_t ncolor = 1;
+    int64_t maxdeg_global = 0;  // largest degree in class 6
+};
+
+static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors, int64_t numColor,
+                          Buckets &b) {
+    const int64_t nv = g->nv;
+    const int64_t nb = numColor * NCLS;
+    b.ncolor = numColor;
+    DevBuf<int32_t> key(ctx, nv);
+    DevBuf<int32_t> counts(ctx, nb);
+    DevBuf<unsigned long long> maxdeg(ctx, 1);
+    VG_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int32_t) * nb, ctx->stream));
+    VG_CUDA(cudaMemsetAsync(maxdeg.p, 0, sizeof(unsigned long long), ctx->stream));
+    if (nv) {
+        LaunchTimer lt(ctx);
+        k_bucket_keys<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(
+            g->rowptr, nv, colors, numColor, key.p, counts.p, maxdeg.p);
+    }
+    VG_CHECK_LAUNCH();
+    std::vector<int32_t> hc(nb);
+    unsigned long long hmax = 0;
+    VG_CUDA(cudaMemcpyAsync(hc.data(), counts.p, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    VG_CUDA(cudaMemcpyAsync(&hmax, maxdeg.p, sizeof(hmax), cudaMemcpyDeviceToHost, ctx->stream));
+    vg_sync(ctx);
+    b.maxdeg_global = (int64_t)hmax;
+    b.start.assign(nb + 1, 0);
+    std::vector<int32_t> fill(nb);
+    for (int64_t k = 0; k < nb; k++) {
+        fill[k] = (int32_t)b.start[k];
+        b.start[k + 1] = b.start[k] + hc[k];
+    }
+    VG_CUDA(cudaMemcpyAsync(counts.p, fill.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice,
+                            ctx->stream));
+    b.list.alloc(ctx, nv);
+    if (nv) {
+        LaunchTimer lt(ctx);
+        k_bucket_scatter<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(nv, key.p, counts.p,
+                                                                          b.list.p);
+    }
+    VG_CHECK_LAUNCH();
+    vg_sync(ctx); // keep `fill` alive until the copy is done
+}
+
+static size_t warp_smem_bytes() {
+    return (size_t)WT_WARPS * WT_CAP * (sizeof(double) + sizeof(int32_t)) +
+           (size_t)WT_WARPS * 32 * sizeof(double);
+}
+static size_t cta_smem_bytes() { return (size_t)CT_CAP * (sizeof(double) + sizeof(int32_t)); }
+
+static void configure_kernels_once() {
+    static bool done = false;
+    if (done) return;
+    VG_CUDA(cudaFuncSetAttribute(k_sweep_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)warp_smem_bytes()));
+    VG_CUDA(cudaFuncSetAttribute(k_sweep_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_smem_bytes()));
+    done = true;
+}
+
+struct GlobalTable {
+    DevBuf<int32_t> keys;
+    DevBuf<double> vals;
+    int64_t cap = 0;
+    int blocks = 0;
+};
+
+// launch the sweep kernels over the lists of one color bucket
+static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64_t color,
+                        GlobalTable &gt) {
+    const int32_t *list = b.list.p;
+    for (int cls = 0; cls < NCLS; cls++) {
+        const int64_t s = b.start[color * NCLS + cls], e = b.start[color * NCLS + cls + 1];
+        const int64_t n = e - s;
+        if (n == 0) continue;
+        LaunchTimer lt(ctx);
+        switch (cls) {
+        case 0: k_sweep_group<4><<<vg_grid(ctx, n * 4, 256, 8), 256, 0, ctx->stream>>>(a, list + s, n); break;
+        case 1: k_sweep_group<8><<<vg_grid(ctx, n * 8, 256, 8), 256, 0, ctx->stream>>>(a, list + s, n); break;
+        case 2: k_sweep_group<16><<<vg_grid(ctx, n * 16, 256, 8), 256, 0, ctx->stream>>>(a, list + s, n); break;
+        case 3: k_sweep_group<32><<<vg_grid(ctx, n * 32, 256, 8), 256, 0, ctx->stream>>>(a, list + s, n); break;
+        case 4:
+            k_sweep_warp<<<vg_grid(ctx, n * 32, WT_WARPS * 32, 4), WT_WARPS * 32, warp_smem_bytes(),
+                           ctx->stream>>>(a, list + s, n);
+            break;
+        case 5:
+            k_sweep_cta<false><<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, 2), CT_THREADS,
+                                 cta_smem_bytes(), ctx->stream>>>(a, list + s, n, nullptr, nullptr, 0);
+            break;
+        default: {
+            const int blocks = (int)std::min<int64_t>(n, gt.blocks);
+            k_sweep_cta<true><<<blocks, CT_THREADS, 0, ctx->stream>>>(a, list + s, n, gt.keys.p,
+                                                                      gt.vals.p, gt.cap);
+        }
+        }
+        VG_CHECK_LAUNCH();
+    }
+}
+
+struct PhaseTiming {
+    double sweep_ms = 0.0;
+    int64_t edges = 0;
+};
+
+// the phase proper; returns the communities in g->comm
+static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double *mod_out,
+                      int32_t *iters_out, PhaseTiming *timing) {
+    configure_kernels_once();
+    const int64_t nv = g->nv;
+    int ordering = p->ordering;
+    int et = p->et_type;
+    VG_REQUIRE(et >= 0 && et <= 4, "early-termination type must be 0..4 (got %d)", et);
+    VG_REQUIRE(ordering >= 0 && ordering <= 2, "ordering must be 0, 1 or 2 (got %d)", ordering);
+    int64_t numColor = 1;
+    if (ordering != 0) {
+        VG_REQUIRE(g->colors != nullptr && g->num_colors >= 0,
+                   "ordering %d needs a coloring (vg_color or vg_set_colors)", ordering);
+        numColor = g->num_colors + 1;
+        if (numColor == 1) { // louvain.cpp:600-605: plain fallback without early termination
+            ordering = 0;
+            et = 0;
+        }
+    }
+    const bool use_et = et != 0;
+    DevBuf<double> vdeg(ctx, nv), cdeg(ctx, nv), udeg(ctx, nv), cw(ctx, nv);
+    DevBuf<int32_t> csize(ctx, nv), usize(ctx, nv);
+    DevBuf<int32_t> A(ctx, nv), B(ctx, nv), C(ctx, nv);
+    DevBuf<double> frozen, pA, pB;
+    DevBuf<uint8_t> active;
+    if (use_et) {
+        frozen.alloc(ctx, nv);
+        active.alloc(ctx, nv);
+        if (et == 2 || et == 4) {
+            pA.alloc(ctx, nv);
+            pB.alloc(ctx, nv);
+        }
+    }
+    const int grid = vg_grid(ctx, nv, 256);
+    if (nv) {
+        {
+            LaunchTimer lt(ctx);
+            k_degree<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->weight, nv, vdeg.p);
+        }
+        VG_CHECK_LAUNCH();
+    }
+    const double twice_m = nv ? vg_sum_f64(ctx, vdeg.p, nv) : 0.0;
+    const double constant = 1.0 / twice_m; // distCalcConstantForSecondTerm (louvain.cpp:2217)
+    if (nv) {
+        LaunchTimer lt(ctx);
+        k_init<<<grid, 256, 0, ctx->stream>>>(nv, vdeg.p, cdeg.p, csize.p, udeg.p, usize.p, A.p, B.p,
+                                              C.p, active.p, pA.p, pB.p);
+    }
+    VG_CHECK_LAUNCH();
+    Buckets bk;
+    build_buckets(ctx, g, ordering ? g->colors : nullptr, numColor, bk);
+    GlobalTable gt;
+    if (bk.maxdeg_global > 0) {
+        int64_t cap = 32;
+        while (cap < 2 * bk.maxdeg_global) cap <<= 1;
+        int64_t n6 = 0;
+        for (int64_t c = 0; c < numColor; c++) n6 = std::max(n6, bk.start[c * NCLS + 7] - bk.start[c * NCLS + 6]);
+        gt.blocks = (int)std::min<int64_t>(n6, (int64_t)ctx->sm_count * 2);
+        gt.cap = cap;
+        gt.keys.alloc(ctx, (size_t)cap * gt.blocks);
+        gt.vals.alloc(ctx, (size_t)cap * gt.blocks);
+    }
+    DevBuf<double> part(ctx, 3 * APPLY_BLOCKS);
+    DevBuf<double> modv(ctx, 4);
+    double *hmod = (double *)vg_pinned(ctx, 4 * sizeof(double));
+
+    int32_t *past = A.p, *curr = B.p, *target = C.p;
+    double *pcurr = pA.p, *pprev = pB.p;
+    double prevMod = p->lower, currMod = -1.0;
+    const double lower = p->lower;
+    int numIters = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (timing) {
+        VG_CUDA(cudaEventCreate(&ev0));
+        VG_CUDA(cudaEventCreate(&ev1));
+    }
+    for (;;) {
+        numIters++;
+        SweepArgs a;
+        a.rowptr = g->rowptr;
+        a.tail = g->tail;
+        a.weight = g->weight;
+        a.curr = curr;
+        a.target = target;
+        a.vdeg = vdeg.p;
+        a.cdeg = cdeg.p;
+        a.csize = csize.p;
+        a.udeg = udeg.p;
+        a.usize = usize.p;
+        a.cw = cw.p;
+        a.frozen = frozen.p;
+        a.active = use_et ? active.p : nullptr;
+        a.constant = constant;
+        if (timing) VG_CUDA(cudaEventRecord(ev0, ctx->stream));
+        for (int64_t ci = 0; ci < numColor; ci++) {
+            sweep_color(ctx, a, bk, ci, gt);
+            if (ordering == 1 && nv) { // per-color community update (louvain.cpp:724-735)
+                LaunchTimer lt(ctx);
+                k_apply_mod<<<APPLY_BLOCKS, APPLY_THREADS, 0, ctx->stream>>>(
+                    nv, cdeg.p, csize.p, udeg.p, usize.p, cw.p, a.active, 0, part.p);
+                VG_CHECK_LAUNCH();
+            }
+        }
+        if (timing) VG_CUDA(cudaEventRecord(ev1, ctx->stream));
+        if (nv) {
+            {
+                LaunchTimer lt(ctx);
+                k_apply_mod<<<APPLY_BLOCKS, APPLY_THREADS, 0, ctx->stream>>>(
+                    nv, cdeg.p, csize.p, udeg.p, usize.p, cw.p, a.active, 1, part.p);
+            }
+            VG_CHECK_LAUNCH();
+            {
+                LaunchTimer lt(ctx);
+                k_mod_final<<<1, 512, 0, ctx->stream>>>(part.p, APPLY_BLOCKS, constant, modv.p);
+            }
+            VG_CHECK_LAUNCH();
+            VG_CUDA(cudaMemcpyAsync(hmod, modv.p, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+        } else {
+            hmod[0] = NAN;
+            hmod[1] = 0.0;
+        }
+        vg_sync(ctx);
+        if (timing) {
+            float ms = 0.f;
+            VG_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+            timing->sweep_ms += ms;
+            timing->edges += g->ne;
+        }
+        if (et == 3 || et == 4) { // ETLocalOrRemote == false (louvain.cpp:112-121)
+            if ((long)hmod[1] >= 90) { // ET_CUTOFF (louvain.hpp:70)
+                currMod = -1;
+                break;
+            }
+        }
+        currMod = hmod[0];
+        if ((currMod - prevMod) < p->threshold) break;
+        prevMod = currMod;
+        if (prevMod < lower) prevMod = lower;
+        if (et == 0) {
+            int32_t *tmp = past; // louvain.cpp:565-570
+            past = curr;
+            curr = target;
+            target = tmp;
+        } else if (et == 1 || et == 3) {
+            LaunchTimer lt(ctx);
+            k_swap_et13<<<grid, 256, 0, ctx->stream>>>(nv, numIters, past, curr, target, active.p);
+            VG_CHECK_LAUNCH();
+        } else {
+            {
+                LaunchTimer lt(ctx);
+                k_swap_et24<<<grid, 256, 0, ctx->stream>>>(nv, numIters, 1.0 - p->et_delta, past,
+                                                           curr, target, active.p, pcurr, pprev);
+            }
+            VG_CHECK_LAUNCH();
+            std::swap(pcurr, pprev);
+        }
+    }
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    (void)currMod;
+    // cvect = pastComm (louvain.cpp:579): keep it on the device for the rebuild
+    vg_free(ctx, g->comm, sizeof(int32_t) * nv);
+    g->comm = nullptr;
+    if (past == A.p) g->comm = A.detach();
+    else if (past == B.p) g->comm = B.detach();
+    else g->comm = C.detach();
+    *mod_out = prevMod;
+    *iters_out = numIters;
+}
+
+void vg_phase_internal(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double *mod_out,
+                       int32_t *iters_out, double *sweep_ms, int64_t *edges) {
+    PhaseTiming t;
+    run_phase(ctx, g, p, mod_out, iters_out, sweep_ms ? &t : nullptr);
+    if (sweep_ms) *sweep_ms = t.sweep_ms;
+    if (edges) *edges = t.edges;
+}
+
+void vg_download_comm(vg_ctx *ctx, const int32_t *comm, int64_t n, int64_t *out) {
+    if (!n) return;
+    DevBuf<int64_t> wide(ctx, n);
+    {
+        LaunchTimer lt(ctx);
+        k_widen<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(comm, n, wide.p);
+    }
+    VG_CHECK_LAUNCH();
+    VG_CUDA(cudaMemcpyAsync(out, wide.p, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    vg_sync(ctx);
+}
+
+// host int64 ids -> device int32, each in [-1, lim)
+void vg_upload_ids(vg_ctx *ctx, const int64_t *in, int64_t n, int64_t lim, int32_t *out) {
+    if (!n) return;
+    DevBuf<int64_t> wide(ctx, n);
+    DevBuf<int> bad(ctx, 1);
+    VG_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
+    VG_CUDA(cudaMemcpyAsync(wide.p, in, sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    {
+        LaunchTimer lt(ctx);
+        k_narrow<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(wide.p, n, lim, out, bad.p);
+    }
+    VG_CHECK_LAUNCH();
+    int *hb = (int *)vg_pinned(ctx, sizeof(int));
+    VG_CUDA(cudaMemcpyAsync(hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    vg_sync(ctx);
+    VG_REQUIRE(*hb == 0, "id out of range");
+}
+
+extern "C" vg_status vg_louvain_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p,
+                                      int64_t *cvect_out, double *mod_out, int32_t *iters_out) {
+    if (!ctx || !g || !p || !mod_out || !iters_out) return VG_ERR_ARG;
+    return vg_guard(ctx, [&] {
+        VG_CUDA(cudaSetDevice(ctx->device));
+        run_phase(ctx, g, p, mod_out, iters_out, nullptr);
+        if (cvect_out) vg_download_comm(ctx, g->comm, g->nv, cvect_out);
+    });
+}
+
+extern "C" vg_status vg_vertex_degree(vg_ctx *ctx, vg_graph *g, double *vdeg_out,
+                                      double *constant_out) {
+    if (!ctx || !g) return VG_ERR_ARG;
+    return vg_guard(ctx, [&] {
+        VG_CUDA(cudaSetDevice(ctx->device));
+        DevBuf<double> vdeg(ctx, g->nv);
+        if (g->nv) {
+            LaunchTimer lt(ctx);
+            k_degree<<<vg_grid(ctx, g->nv, 256), 256, 0, ctx->stream>>>(g->rowptr, g->weight, g->nv,
+                                                                         vdeg.p);
+        }
+        VG_CHECK_LAUNCH();
+        const double tm = g->nv ? vg_sum_f64(ctx, vdeg.p, g->nv) : 0.0;
+        if (constant_out) *constant_out = 1.0 / tm;
+        if (vdeg_out && g->nv) {
+            VG_CUDA(cudaMemcpyAsync(vdeg_out, vdeg.p, sizeof(double) * g->nv, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+        }
+        vg_sync(ctx);
+    });
+}

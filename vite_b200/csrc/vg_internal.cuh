@@ -1,0 +1,184 @@
+// Internal declarations shared by the CUDA sources of libvite_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "vite_b200.h"
+
+// ---------------------------------------------------------------------------------
+// error handling
+
+struct vg_error : public std::exception {
+    vg_status status;
+    std::string msg;
+    vg_error(vg_status s, std::string m) : status(s), msg(std::move(m)) {}
+    const char *what() const noexcept override { return msg.c_str(); }
+};
+
+[[noreturn]] void vg_throw(vg_status s, const char *fmt, ...);
+
+#define VG_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t _e = (call);                                                               \
+        if (_e != cudaSuccess)                                                                 \
+            vg_throw(_e == cudaErrorMemoryAllocation ? VG_ERR_OOM : VG_ERR_CUDA, "%s: %s (%s:%d)", \
+                     #call, cudaGetErrorString(_e), __FILE__, __LINE__);                       \
+    } while (0)
+
+#define VG_CHECK_LAUNCH() VG_CUDA(cudaGetLastError())
+
+#define VG_REQUIRE(cond, ...)                                                                  \
+    do {                                                                                       \
+        if (!(cond)) vg_throw(VG_ERR_ARG, __VA_ARGS__);                                        \
+    } while (0)
+
+// ---------------------------------------------------------------------------------
+// context
+
+struct vg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0;        // 0 = unlimited
+    size_t in_use = 0;        // bytes held through vg_alloc
+    std::string last_error;
+    int sm_count = 148;
+    // pinned host staging for small read-backs
+    void *pinned = nullptr;
+    size_t pinned_bytes = 0;
+    // kernel instrumentation (events around each launch when enabled)
+    bool profile = false;
+    double profile_ms = 0.0;
+    int64_t profile_launches = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> event_pool;
+};
+
+// stream-ordered device allocation accounted against the context budget
+void *vg_alloc(vg_ctx *ctx, size_t bytes);
+void vg_free(vg_ctx *ctx, void *p, size_t bytes);
+
+template <class T> struct DevBuf {
+    vg_ctx *ctx = nullptr;
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(vg_ctx *c, size_t count) { alloc(c, count); }
+    void alloc(vg_ctx *c, size_t count) {
+        release();
+        ctx = c;
+        n = count;
+        p = count ? (T *)vg_alloc(c, count * sizeof(T)) : nullptr;
+    }
+    void release() {
+        if (p) vg_free(ctx, p, n * sizeof(T));
+        p = nullptr;
+        n = 0;
+    }
+    T *detach() {
+        T *q = p;
+        p = nullptr;
+        n = 0;
+        return q;
+    }
+    ~DevBuf() { release(); }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : ctx(o.ctx), p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        if (this != &o) { release(); ctx = o.ctx; p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    void swap(DevBuf &o) { std::swap(ctx, o.ctx); std::swap(p, o.p); std::swap(n, o.n); }
+};
+
+// pinned scratch for read-backs of a few scalars
+void *vg_pinned(vg_ctx *ctx, size_t bytes);
+void vg_sync(vg_ctx *ctx);
+
+// launch bracketing for instrumentation
+struct LaunchTimer {
+    vg_ctx *ctx;
+    cudaEvent_t a = nullptr, b = nullptr;
+    explicit LaunchTimer(vg_ctx *c);
+    ~LaunchTimer();
+};
+void vg_profile_collect(vg_ctx *ctx);
+
+// ---------------------------------------------------------------------------------
+// device graph: Vite's CSR with int32 tails and FP64 weights in separate arrays
+
+struct vg_graph {
+    int64_t nv = 0, ne = 0;
+    int64_t *rowptr = nullptr; // nv+1
+    int32_t *tail = nullptr;   // ne
+    double *weight = nullptr;  // ne
+    // coloring attached by vg_color / vg_set_colors (int32, -1 uncolored)
+    int32_t *colors = nullptr;
+    int64_t num_colors = -1;   // reference's nextColor; -1 = none
+    // communities of the last phase (int32), kept for vg_rebuild
+    int32_t *comm = nullptr;
+};
+
+void vg_graph_release(vg_ctx *ctx, vg_graph *g);
+// the graph takes ownership of the three arrays
+vg_graph *vg_graph_wrap(vg_ctx *ctx, int64_t nv, int64_t ne, int64_t *rowptr, int32_t *tail,
+                        double *weight);
+
+// ---------------------------------------------------------------------------------
+// primitives (primitives.cu)
+
+// exclusive scan in place over n elements; returns the total
+int64_t vg_exclusive_scan_i64(vg_ctx *ctx, int64_t *data, int64_t n);
+int64_t vg_exclusive_scan_i32_to_i64(vg_ctx *ctx, const int32_t *in, int64_t *out, int64_t n);
+// stable LSD radix sort of 64-bit keys with 32-bit payloads over the low `bits` bits
+void vg_radix_sort_pairs(vg_ctx *ctx, uint64_t *keys, uint32_t *vals, int64_t n, int bits);
+// sum of a double array (deterministic)
+double vg_sum_f64(vg_ctx *ctx, const double *x, int64_t n);
+
+// CSR from (src, dst, w) triples in their given order: stable sort by (src, dst),
+// adjacent duplicates combined by summing their weights in order when `combine`.
+// nv rows; the three inputs are consumed (freed).
+vg_graph *vg_csr_from_triples(vg_ctx *ctx, int64_t nv, DevBuf<int32_t> &src,
+                              DevBuf<int32_t> &dst, DevBuf<double> &w, int64_t m, bool combine);
+
+// ---------------------------------------------------------------------------------
+// kernels shared across files
+
+int vg_grid(vg_ctx *ctx, int64_t work, int block, int per_sm = 8);
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31; }
+
+// counter-based generator shared with the oracle's restatement
+__host__ __device__ __forceinline__ uint64_t vg_sm64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return x ^ (x >> 31);
+}
+__host__ __device__ __forceinline__ uint64_t vg_mix(uint64_t seed, uint64_t stream, uint64_t k) {
+    return vg_sm64(vg_sm64(seed ^ (stream * 0xD1B54A32D192ED03ULL)) ^ k);
+}
+__device__ __forceinline__ uint64_t vg_uint_below(uint64_t r, uint64_t n) { return __umul64hi(r, n); }
+__device__ __forceinline__ double vg_unit_double(uint64_t r) {
+    return __dmul_rn((double)(r >> 11), 1.0 / 9007199254740992.0);
+}
+
+// entry-point wrapper: converts exceptions into a status + message
+template <class F> vg_status vg_guard(vg_ctx *ctx, F &&f) {
+    try {
+        f();
+        return VG_OK;
+    } catch (const vg_error &e) {
+        if (ctx) ctx->last_error = e.msg;
+        return e.status;
+    } catch (const std::exception &e) {
+        if (ctx) ctx->last_error = e.what();
+        return VG_ERR_CUDA;
+    }
+}
