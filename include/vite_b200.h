@@ -64,6 +64,10 @@ typedef struct vg_run_params {
     double et_delta;           /* -a */
     int32_t threshold_scaling; /* -i */
     int32_t one_phase;         /* -p */
+    int32_t layout;            /* HBM layout of the level-0 graph: 0 as given, 1 locality order
+                                  computed on the device (vg_graph_reorder mode 1), 2 locality
+                                  order when the graph has at least 2^18 vertices. Results are
+                                  the same in every layout. */
 } vg_run_params;
 
 /* What graphClustering prints per level (main.cpp:465-474), measured on the device. */
@@ -77,6 +81,7 @@ typedef struct vg_level_stat {
     double seconds_sweep;      /* device time of the local-moving sweeps alone */
     double seconds_rebuild;    /* device time of the rebuild after the level (0 if none) */
     int64_t edges_swept;       /* sum over iterations of the edges the sweeps visited */
+    double seconds_layout;     /* device time of the level-0 layout step (0 if none) */
 } vg_level_stat;
 
 /* --- context ---------------------------------------------------------------- */
@@ -109,6 +114,14 @@ vg_status vg_graph_info(const vg_graph *g, int64_t *nv, int64_t *ne);
  * distgraph.cpp:986-1064). rowptr has nv+1 entries, edges ne. */
 vg_status vg_graph_download(vg_ctx *ctx, const vg_graph *g, int64_t *rowptr, vg_edge *edges);
 vg_status vg_graph_free(vg_ctx *ctx, vg_graph *g);
+
+/* Store the graph in another vertex order on the device (no reference
+ * counterpart: the reference keeps its input order). mode 1: locality order
+ * (multi-source BFS clusters) so that a sweep's gathers stay in few cache
+ * lines; mode 0: back to reference order. Ids at the boundary stay the
+ * reference's in every layout and every result is unchanged; the communities
+ * and colors attached to g are dropped. */
+vg_status vg_graph_reorder(vg_ctx *ctx, vg_graph *g, int32_t mode);
 
 /* distSumVertexDegree + distCalcConstantForSecondTerm (louvain.cpp:2161-2218):
  * weighted degree of every vertex (optional copy out) and 1/(2m). */

@@ -138,6 +138,44 @@ def test_levels_bit_identical_unit_weights(ctx, golden, name):
         assert digest(got.cvect.astype("<i8")) == ref["cvect"]
 
 
+@pytest.mark.parametrize("name", ["rgg4k_unit", "rgg64k_unit", "rgg4k_unit_c8", "ba4k_c8_t2",
+                                  "ba4k_t1", "ba4k_t4", "ba4k_d8", "er4k"])
+def test_levels_bit_identical_in_locality_layout(ctx, golden, name):
+    """The same per-level results when the graph is stored in the locality layout."""
+    import vite_b200
+    e = golden[name]
+    g = upload(ctx, vo.golden_graph(e))
+    ctx.reorder(g, 1)
+    levels = vite_b200.run_levels(ctx, g, **vo.flags_to_kwargs(e["flags"]))
+    assert len(levels) == len(e["levels"])
+    for got, ref in zip(levels, e["levels"]):
+        assert (got.nv, got.ne, got.iters) == (ref["nv"], ref["ne"], ref["iters"])
+        assert float(got.mod).hex() == ref["mod"]
+        assert digest(got.cvect.astype("<i8")) == ref["cvect"]
+
+
+def test_layout_roundtrip_and_rebuild(ctx):
+    gref = vo.rgg(65536)
+    g = upload(ctx, gref)
+    ctx.reorder(g, 1)
+    assert_graph_equal(g.download(), gref)  # downloads come back in reference order
+    cv, mod, it = ctx.louvain_phase(g)
+    rcv, rmod, rit = vo.louvain_phase(gref)
+    np.testing.assert_array_equal(cv, rcv)
+    ctx.rebuild(g)
+    assert_graph_equal(g.download(), vo.rebuild(gref, rcv))
+    ctx.reorder(g, 0)
+    assert_graph_equal(g.download(), vo.rebuild(gref, rcv))
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_run_layouts_match_golden(ctx, golden, layout):
+    e = golden["rgg64k_unit"]
+    res = ctx.run(upload(ctx, vo.golden_graph(e)), layout=layout)
+    assert [float(s["modularity"]).hex() for s in res.stats] == [lv["mod"] for lv in e["levels"]]
+    assert [s["iters"] for s in res.stats] == [lv["iters"] for lv in e["levels"]]
+
+
 @pytest.mark.parametrize("name", ["rgg4k", "rgg64k", "rgg4k_c8_t2", "rgg16k_extra"])
 def test_levels_real_weights(ctx, golden, name):
     """Real weights: per-level modularity within REL_TOL of the reference."""

@@ -34,6 +34,7 @@ EXPORTED_SYMBOLS = [
     "vg_graph_upload", "vg_graph_info", "vg_graph_download", "vg_graph_free", "vg_vertex_degree",
     "vg_louvain_phase", "vg_color", "vg_set_colors", "vg_rebuild", "vg_louvain_run",
     "vg_generate_rgg", "vg_generate_ba", "vg_generate_er", "vg_graph_reweight",
+    "vg_graph_reorder",
 ]
 
 
@@ -52,7 +53,8 @@ class RunParams(C.Structure):
     _fields_ = [("threshold", C.c_double), ("coloring", C.c_int32), ("vertex_order", C.c_int32),
                 ("max_colors", C.c_int32), ("single_color_iter", C.c_int32),
                 ("et_type", C.c_int32), ("et_delta", C.c_double),
-                ("threshold_scaling", C.c_int32), ("one_phase", C.c_int32)]
+                ("threshold_scaling", C.c_int32), ("one_phase", C.c_int32),
+                ("layout", C.c_int32)]
 
 
 class LevelStat(C.Structure):
@@ -60,7 +62,7 @@ class LevelStat(C.Structure):
                 ("modularity", C.c_double), ("num_colors", C.c_int64),
                 ("seconds_color", C.c_double), ("seconds_phase", C.c_double),
                 ("seconds_sweep", C.c_double), ("seconds_rebuild", C.c_double),
-                ("edges_swept", C.c_int64)]
+                ("edges_swept", C.c_int64), ("seconds_layout", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -108,6 +110,7 @@ def lib() -> C.CDLL:
         L.vg_generate_ba.argtypes = [vp, C.c_int64, C.c_int64, C.c_uint64, C.POINTER(vp)]
         L.vg_generate_er.argtypes = [vp, C.c_int64, C.c_double, C.c_uint64, C.POINTER(vp)]
         L.vg_graph_reweight.argtypes = [vp, vp, C.c_int32, C.c_uint64]
+        L.vg_graph_reorder.argtypes = [vp, vp, C.c_int32]
         for name in EXPORTED_SYMBOLS:
             if name not in ("vg_last_error", "vg_ctx_bytes_in_use"):
                 getattr(L, name).restype = C.c_int
@@ -251,6 +254,10 @@ class Context:
         self._check(lib().vg_generate_er(self.handle, n, avg_degree, seed, C.byref(h)))
         return Graph(self, h)
 
+    def reorder(self, g: Graph, mode: int = 1) -> None:
+        """Store g in the locality layout (mode 1) or back in reference order (mode 0)."""
+        self._check(lib().vg_graph_reorder(self.handle, g.handle, mode))
+
     def reweight(self, g: Graph, mode: int, seed: int = 0) -> None:
         self._check(lib().vg_graph_reweight(self.handle, g.handle, mode, seed))
 
@@ -290,10 +297,11 @@ class Context:
     def run(self, g: Graph, threshold: float = 1e-6, coloring: bool = False,
             vertex_order: bool = False, max_colors: int = 8, single_color_iter: bool = False,
             et_type: int = 0, et_delta: float = 1.0, threshold_scaling: bool = False,
-            one_phase: bool = False, want_comm: bool = False, max_levels: int = 256) -> Levels:
+            one_phase: bool = False, want_comm: bool = False, max_levels: int = 256,
+            layout: int = 2) -> Levels:
         p = RunParams(threshold, int(coloring), int(vertex_order), max_colors,
                       int(single_color_iter), et_type, et_delta, int(threshold_scaling),
-                      int(one_phase))
+                      int(one_phase), layout)
         stats = (LevelStat * max_levels)()
         n = C.c_int32()
         comm = np.empty(g.nv, np.int64) if want_comm else None

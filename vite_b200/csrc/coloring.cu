@@ -24,15 +24,18 @@ __host__ __device__ __forceinline__ uint32_t color_hash(uint32_t a, uint32_t see
 // colored concurrently in this round gives the same decision as reading -1
 __global__ void k_color_round(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
                               int64_t nv, int32_t *__restrict__ color, int nHash, int64_t nextColor,
-                              uint32_t seed, unsigned long long *__restrict__ ncolored) {
+                              uint32_t seed, unsigned long long *__restrict__ ncolored,
+                              const int32_t *__restrict__ ref) {
     unsigned long long mine = 0;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
          v += (int64_t)gridDim.x * blockDim.x) {
         if (color[v] != -1) continue;
+        // hashes and the color pick use reference ids (v + base of the reference)
+        const int64_t rv = vg_rid(ref, (int32_t)v);
         int64_t possible = 2 * (int64_t)nHash;
         uint32_t vHash[MAX_HASH];
         for (int t = 0; t < nHash; t++)
-            vHash[t] = color_hash((uint32_t)v, (uint32_t)((int64_t)seed + 1043 * (int64_t)t));
+            vHash[t] = color_hash((uint32_t)rv, (uint32_t)((int64_t)seed + 1043 * (int64_t)t));
         uint32_t not_min = 0, not_max = 0;
         bool can_color = true;
         const int64_t e1 = rowptr[v + 1];
@@ -42,7 +45,8 @@ __global__ void k_color_round(const int64_t *__restrict__ rowptr, const int32_t 
             const int32_t cu = color[u];
             if (cu != -1 && cu < nextColor) continue;
             for (int t = 0; t < nHash; t++) {
-                const uint32_t j = color_hash((uint32_t)u, (uint32_t)((int64_t)seed + 1043 * (int64_t)t));
+                const uint32_t j = color_hash((uint32_t)vg_rid(ref, u),
+                                              (uint32_t)((int64_t)seed + 1043 * (int64_t)t));
                 if (vHash[t] <= j && !(not_max & (1u << t))) {
                     not_max |= (1u << t);
                     possible--;
@@ -58,7 +62,7 @@ __global__ void k_color_round(const int64_t *__restrict__ rowptr, const int32_t 
             }
         }
         if (can_color) {
-            const int64_t col_id = v % possible;
+            const int64_t col_id = rv % possible;
             int64_t this_col = 0;
             for (int t = 0; t < nHash; t++) {
                 if (!(not_min & (1u << t)) && col_id == this_col) {
@@ -115,7 +119,7 @@ int64_t vg_color_internal(vg_ctx *ctx, vg_graph *g, int64_t nHash, int32_t targe
         if (nv) {
             LaunchTimer lt(ctx);
             k_color_round<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(
-                g->rowptr, g->tail, nv, g->colors, (int)nHash, nextColor, seed, cnt.p);
+                g->rowptr, g->tail, nv, g->colors, (int)nHash, nextColor, seed, cnt.p, g->ref);
         }
         VG_CHECK_LAUNCH();
         VG_CUDA(cudaMemcpyAsync(h, cnt.p, sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
@@ -138,7 +142,7 @@ extern "C" vg_status vg_color(vg_ctx *ctx, vg_graph *g, int64_t n_hash, int32_t 
         VG_CUDA(cudaSetDevice(ctx->device));
         const int64_t nc = vg_color_internal(ctx, g, n_hash, target_percent, single_iteration);
         if (num_colors_out) *num_colors_out = nc;
-        if (colors_out) vg_download_comm(ctx, g->colors, g->nv, colors_out);
+        if (colors_out) vg_download_vals_ref(ctx, g, g->colors, colors_out);
     });
 }
 
@@ -150,6 +154,7 @@ extern "C" vg_status vg_set_colors(vg_ctx *ctx, vg_graph *g, const int64_t *colo
         VG_REQUIRE(num_colors >= 0 && num_colors < INT32_MAX, "bad number of colors");
         if (!g->colors) g->colors = (int32_t *)vg_alloc(ctx, sizeof(int32_t) * (g->nv ? g->nv : 1));
         vg_upload_ids(ctx, colors, g->nv, num_colors + 1, g->colors);
+        vg_ref_to_pos_inplace(ctx, g, g->colors, false);
         g->num_colors = num_colors;
     });
 }

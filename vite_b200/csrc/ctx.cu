@@ -182,6 +182,10 @@ void vg_graph_release(vg_ctx *ctx, vg_graph *g) {
     vg_free(ctx, g->weight, sizeof(double) * g->ne);
     vg_free(ctx, g->colors, sizeof(int32_t) * g->nv);
     vg_free(ctx, g->comm, sizeof(int32_t) * g->nv);
+    vg_free(ctx, g->ref, sizeof(int32_t) * g->nv);
+    vg_free(ctx, g->pos, sizeof(int32_t) * g->nv);
+    g->ref = nullptr;
+    g->pos = nullptr;
     g->rowptr = nullptr;
     g->tail = nullptr;
     g->weight = nullptr;
@@ -263,11 +267,24 @@ extern "C" vg_status vg_graph_info(const vg_graph *g, int64_t *nv, int64_t *ne) 
     return VG_OK;
 }
 
-extern "C" vg_status vg_graph_download(vg_ctx *ctx, const vg_graph *g, int64_t *rowptr,
+extern "C" vg_status vg_graph_download(vg_ctx *ctx, const vg_graph *g_in, int64_t *rowptr,
                                        vg_edge *edges) {
-    if (!ctx || !g) return VG_ERR_ARG;
+    if (!ctx || !g_in) return VG_ERR_ARG;
     return vg_guard(ctx, [&] {
         VG_CUDA(cudaSetDevice(ctx->device));
+        // a graph stored in the library's own layout goes out in reference order
+        vg_graph *tmp = g_in->ref ? vg_remove_layout(ctx, g_in) : nullptr;
+        const vg_graph *g = tmp ? tmp : g_in;
+        struct Drop {
+            vg_ctx *c;
+            vg_graph *t;
+            ~Drop() {
+                if (t) {
+                    vg_graph_release(c, t);
+                    delete t;
+                }
+            }
+        } drop{ctx, tmp};
         if (rowptr)
             VG_CUDA(cudaMemcpyAsync(rowptr, g->rowptr, sizeof(int64_t) * (g->nv + 1),
                                     cudaMemcpyDeviceToHost, ctx->stream));
@@ -284,7 +301,6 @@ extern "C" vg_status vg_graph_download(vg_ctx *ctx, const vg_graph *g, int64_t *
                 VG_CHECK_LAUNCH();
                 VG_CUDA(cudaMemcpyAsync(edges + off, stage.p, sizeof(vg_edge) * len,
                                         cudaMemcpyDeviceToHost, ctx->stream));
-                vg_sync(ctx);
             }
         }
         vg_sync(ctx);

@@ -1,0 +1,286 @@
+// HBM layout of a level graph.
+//
+// The reference numbers vertices by its input (for the in-memory RGG: LCG order,
+// which is random in space), so the gathers of a sweep (community of every
+// neighbour, degree of every candidate community) hit random cache lines. The
+// library may therefore store a graph in its own vertex order ("positions"):
+// position p holds the vertex whose reference id is ref[p] (pos is the inverse).
+// Rows keep the reference's CSR order of their entries, so every sum is the same
+// left fold; every comparison of ids (tie-breaks, the singleton rule, the
+// early-termination test, coloring hashes, first-appearance numbering in the
+// rebuild) is made on reference ids, so results are identical to the
+// reference's. Only the addresses change.
+//
+// The locality order is computed on the device from the graph alone: a
+// multi-source breadth-first search from hashed seeds (about one seed per 1024
+// vertices) labels each vertex with its nearest seed, and vertices are ordered by
+// (seed, BFS distance, id), so a cluster occupies a contiguous range of positions
+// and most neighbours of a vertex lie in the same few cache lines.
+#include "vg_internal.cuh"
+
+#include <algorithm>
+
+namespace {
+
+constexpr int SEED_SHIFT = 10; // one seed per 2^10 vertices on average
+constexpr int MAX_BFS_STEPS = 255;
+
+__global__ void k_bfs_init(int64_t nv, uint64_t seed, int32_t *__restrict__ label,
+                           uint8_t *__restrict__ dist) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const bool s = (vg_mix(seed, 41, (uint64_t)v) & ((1ULL << SEED_SHIFT) - 1)) == 0;
+        label[v] = s ? (int32_t)v : -1;
+        dist[v] = s ? 0 : 255;
+    }
+}
+
+// one level: vertices at distance step-1 claim their unlabeled neighbours
+__global__ void k_bfs_step(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
+                           int64_t nv, int step, int32_t *__restrict__ label,
+                           uint8_t *__restrict__ dist, unsigned long long *__restrict__ claimed) {
+    unsigned long long mine = 0;
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < nv;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        if (dist[u] != step - 1) continue;
+        const int32_t lu = label[u];
+        const int64_t e1 = rowptr[u + 1];
+        for (int64_t e = rowptr[u]; e < e1; e++) {
+            const int32_t w = tail[e];
+            if (label[w] == -1 && atomicCAS(&label[w], -1, lu) == -1) {
+                dist[w] = (uint8_t)step;
+                mine++;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, o);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(claimed, mine);
+}
+
+__global__ void k_order_keys(int64_t nv, const int32_t *__restrict__ label,
+                             const uint8_t *__restrict__ dist, uint64_t *__restrict__ keys,
+                             uint32_t *__restrict__ vals) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t l = label[v];
+        // unreached vertices (components without a seed) keep their own place
+        keys[v] = l < 0 ? ((uint64_t)v << 8) : (((uint64_t)l << 8) | dist[v]);
+        vals[v] = (uint32_t)v;
+    }
+}
+
+__global__ void k_inverse(const int32_t *__restrict__ perm, int64_t n, int32_t *__restrict__ inv) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x)
+        inv[perm[k]] = (int32_t)k;
+}
+
+__global__ void k_gather_deg(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ from,
+                             int64_t n, int64_t *__restrict__ deg) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t r = from[k];
+        deg[k] = rowptr[r + 1] - rowptr[r];
+    }
+}
+
+// new row k = old row from[k], tails renamed through `rename`, entry order kept
+__global__ void k_move_rows(const int64_t *__restrict__ rp, const int32_t *__restrict__ tail,
+                            const double *__restrict__ w, int64_t n, const int32_t *__restrict__ from,
+                            const int32_t *__restrict__ rename, const int64_t *__restrict__ rp2,
+                            int32_t *__restrict__ tail2, double *__restrict__ w2) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t k = wg; k < n; k += nw) {
+        const int32_t r = from[k];
+        const int64_t s = rp[r], len = rp[r + 1] - s, o = rp2[k];
+        for (int64_t j = lane; j < len; j += 32) {
+            tail2[o + j] = rename[tail[s + j]];
+            w2[o + j] = w[s + j];
+        }
+    }
+}
+
+__global__ void k_copy_i32(const int32_t *__restrict__ a, int64_t n, int32_t *__restrict__ b) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x)
+        b[k] = a[k];
+}
+
+// community vector of positions -> reference ids, indexed by reference vertex id
+__global__ void k_comm_to_ref(const int32_t *__restrict__ comm, int64_t n,
+                              const int32_t *__restrict__ ref, int64_t *__restrict__ out) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x)
+        out[ref[p]] = ref[comm[p]];
+}
+
+// per-vertex values (colors) in position order -> reference order
+__global__ void k_vals_to_ref(const int32_t *__restrict__ x, int64_t n,
+                              const int32_t *__restrict__ ref, int64_t *__restrict__ out) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x)
+        out[ref[p]] = x[p];
+}
+
+// reference-ordered int32 values -> position order; `rename` maps the values too
+__global__ void k_ref_to_pos(const int32_t *__restrict__ in, int64_t n,
+                             const int32_t *__restrict__ ref, const int32_t *__restrict__ rename,
+                             int32_t *__restrict__ out) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t x = in[ref[p]];
+        out[p] = (rename && x >= 0) ? rename[x] : x;
+    }
+}
+
+} // namespace
+
+int64_t vg_exclusive_scan_i64(vg_ctx *ctx, int64_t *data, int64_t n);
+
+// graph with rows in `from` order; tails renamed through `rename`
+static vg_graph *move_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *from,
+                           const int32_t *rename) {
+    const int64_t nv = g->nv, ne = g->ne;
+    DevBuf<int64_t> rp(ctx, nv + 1);
+    VG_CUDA(cudaMemsetAsync(rp.p + nv, 0, sizeof(int64_t), ctx->stream));
+    if (nv) {
+        LaunchTimer lt(ctx);
+        k_gather_deg<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(g->rowptr, from, nv, rp.p);
+    }
+    VG_CHECK_LAUNCH();
+    vg_exclusive_scan_i64(ctx, rp.p, nv + 1);
+    DevBuf<int32_t> tail(ctx, ne);
+    DevBuf<double> w(ctx, ne);
+    if (nv) {
+        LaunchTimer lt(ctx);
+        k_move_rows<<<vg_grid(ctx, nv * 32, 256), 256, 0, ctx->stream>>>(
+            g->rowptr, g->tail, g->weight, nv, from, rename, rp.p, tail.p, w.p);
+    }
+    VG_CHECK_LAUNCH();
+    return vg_graph_wrap(ctx, nv, ne, rp.detach(), tail.detach(), w.detach());
+}
+
+void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
+    const int64_t nv = g->nv;
+    order.alloc(ctx, nv);
+    if (!nv) return;
+    DevBuf<int32_t> label(ctx, nv);
+    DevBuf<uint8_t> dist(ctx, nv);
+    DevBuf<unsigned long long> claimed(ctx, 1);
+    unsigned long long *h = (unsigned long long *)vg_pinned(ctx, sizeof(unsigned long long));
+    const int grid = vg_grid(ctx, nv, 256);
+    { LaunchTimer lt(ctx); k_bfs_init<<<grid, 256, 0, ctx->stream>>>(nv, 0x5eedULL, label.p, dist.p); }
+    VG_CHECK_LAUNCH();
+    for (int step = 1; step <= MAX_BFS_STEPS - 1; step++) {
+        VG_CUDA(cudaMemsetAsync(claimed.p, 0, sizeof(unsigned long long), ctx->stream));
+        { LaunchTimer lt(ctx);
+          k_bfs_step<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->tail, nv, step, label.p, dist.p,
+                                                    claimed.p); }
+        VG_CHECK_LAUNCH();
+        VG_CUDA(cudaMemcpyAsync(h, claimed.p, sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
+        vg_sync(ctx);
+        if (*h == 0) break;
+    }
+    DevBuf<uint64_t> keys(ctx, nv);
+    DevBuf<uint32_t> vals(ctx, nv);
+    { LaunchTimer lt(ctx); k_order_keys<<<grid, 256, 0, ctx->stream>>>(nv, label.p, dist.p, keys.p, vals.p); }
+    VG_CHECK_LAUNCH();
+    int bits = 1;
+    while (bits < 40 && ((int64_t)1 << bits) < nv) bits++;
+    vg_radix_sort_pairs(ctx, keys.p, vals.p, nv, bits + 8);
+    VG_CUDA(cudaMemcpyAsync(order.p, vals.p, sizeof(int32_t) * nv, cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+}
+
+// g in reference layout -> the same graph stored in `order` (order[p] = reference id)
+vg_graph *vg_apply_layout(vg_ctx *ctx, const vg_graph *g, const int32_t *order) {
+    VG_REQUIRE(g->ref == nullptr, "graph already has a layout");
+    const int64_t nv = g->nv;
+    DevBuf<int32_t> pos(ctx, nv), ref(ctx, nv);
+    if (nv) {
+        { LaunchTimer lt(ctx); k_inverse<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(order, nv, pos.p); }
+        VG_CHECK_LAUNCH();
+        { LaunchTimer lt(ctx); k_copy_i32<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(order, nv, ref.p); }
+        VG_CHECK_LAUNCH();
+    }
+    vg_graph *h = move_rows(ctx, g, order, pos.p);
+    h->ref = ref.detach();
+    h->pos = pos.detach();
+    return h;
+}
+
+// the graph back in reference layout (rows by reference id, tails as reference ids)
+vg_graph *vg_remove_layout(vg_ctx *ctx, const vg_graph *g) {
+    VG_REQUIRE(g->ref != nullptr, "graph has no layout");
+    return move_rows(ctx, g, g->pos, g->ref);
+}
+
+// device community vector (positions) -> host reference ids indexed by reference id
+void vg_download_comm_ref(vg_ctx *ctx, const vg_graph *g, const int32_t *comm, int64_t *out) {
+    const int64_t n = g->nv;
+    if (!n) return;
+    if (!g->ref) {
+        void vg_download_comm(vg_ctx *, const int32_t *, int64_t, int64_t *);
+        vg_download_comm(ctx, comm, n, out);
+        return;
+    }
+    DevBuf<int64_t> wide(ctx, n);
+    { LaunchTimer lt(ctx);
+      k_comm_to_ref<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(comm, n, g->ref, wide.p); }
+    VG_CHECK_LAUNCH();
+    VG_CUDA(cudaMemcpyAsync(out, wide.p, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    vg_sync(ctx);
+}
+
+void vg_download_vals_ref(vg_ctx *ctx, const vg_graph *g, const int32_t *x, int64_t *out) {
+    const int64_t n = g->nv;
+    if (!n) return;
+    if (!g->ref) {
+        void vg_download_comm(vg_ctx *, const int32_t *, int64_t, int64_t *);
+        vg_download_comm(ctx, x, n, out);
+        return;
+    }
+    DevBuf<int64_t> wide(ctx, n);
+    { LaunchTimer lt(ctx);
+      k_vals_to_ref<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(x, n, g->ref, wide.p); }
+    VG_CHECK_LAUNCH();
+    VG_CUDA(cudaMemcpyAsync(out, wide.p, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    vg_sync(ctx);
+}
+
+// reference-ordered device int32 values -> position order in place (values
+// renamed through pos when `are_ids`)
+void vg_ref_to_pos_inplace(vg_ctx *ctx, const vg_graph *g, int32_t *x, bool are_ids) {
+    if (!g->ref || !g->nv) return;
+    DevBuf<int32_t> tmp(ctx, g->nv);
+    { LaunchTimer lt(ctx);
+      k_ref_to_pos<<<vg_grid(ctx, g->nv, 256), 256, 0, ctx->stream>>>(x, g->nv, g->ref,
+                                                                       are_ids ? g->pos : nullptr, tmp.p); }
+    VG_CHECK_LAUNCH();
+    VG_CUDA(cudaMemcpyAsync(x, tmp.p, sizeof(int32_t) * g->nv, cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+extern "C" vg_status vg_graph_reorder(vg_ctx *ctx, vg_graph *g, int32_t mode) {
+    if (!ctx || !g) return VG_ERR_ARG;
+    return vg_guard(ctx, [&] {
+        VG_CUDA(cudaSetDevice(ctx->device));
+        VG_REQUIRE(mode == 0 || mode == 1, "layout mode must be 0 (reference order) or 1 (locality)");
+        vg_graph *h = nullptr;
+        if (mode == 1 && !g->ref) {
+            DevBuf<int32_t> order;
+            vg_bfs_order(ctx, g, order);
+            h = vg_apply_layout(ctx, g, order.p);
+        } else if (mode == 0 && g->ref) {
+            h = vg_remove_layout(ctx, g);
+        }
+        if (h) {
+            vg_graph_release(ctx, g); // communities and colors of the old layout are dropped
+            *g = *h;
+            delete h;
+        }
+        vg_sync(ctx);
+    });
+}

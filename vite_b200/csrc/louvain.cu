@@ -20,10 +20,12 @@
 
 namespace {
 
-constexpr int NCLS = 7;
-// class by degree: 0:<=4 1:<=8 2:<=16 3:<=32 (sub-warp groups, one chunk)
-// 4:<=WT_MAXDEG (warp, shared-memory table) 5:<=CT_MAXDEG (CTA, shared table)
-// 6: above (CTA, table in global scratch)
+constexpr int NCLS = 5;
+// class by degree: 0: <= TMAX (one thread per vertex) 1: <= 32 (one warp, one chunk)
+// 2: <= WT_MAXDEG (warp, shared-memory table) 3: <= CT_MAXDEG (CTA, shared table)
+// 4: above (CTA, table in global scratch)
+constexpr int TMAX = 16;
+constexpr int TB = 256;
 constexpr int WT_MAXDEG = 512;
 constexpr int WT_CAP = 1024;
 constexpr int WT_WARPS = 4;
@@ -33,14 +35,20 @@ constexpr int CT_THREADS = 256;
 constexpr int32_t EMPTY = -1;
 
 __host__ __device__ __forceinline__ int degree_class(int64_t d) {
-    if (d <= 4) return 0;
-    if (d <= 8) return 1;
-    if (d <= 16) return 2;
-    if (d <= 32) return 3;
-    if (d <= WT_MAXDEG) return 4;
-    if (d <= CT_MAXDEG) return 5;
-    return 6;
+    if (d <= TMAX) return 0;
+    if (d <= 32) return 1;
+    if (d <= WT_MAXDEG) return 2;
+    if (d <= CT_MAXDEG) return 3;
+    return 4;
 }
+
+// community update (localCupdate, Comm of graph.hpp:77-82) packed in 16 bytes so
+// that the four atomics of a move land on two sectors
+struct __align__(16) CommInfo {
+    double deg;
+    int32_t size;
+    int32_t pad;
+};
 
 struct SweepArgs {
     const int64_t *__restrict__ rowptr;
@@ -49,13 +57,13 @@ struct SweepArgs {
     const int32_t *__restrict__ curr;
     int32_t *__restrict__ target;
     const double *__restrict__ vdeg;
-    const double *__restrict__ cdeg;
-    const int32_t *__restrict__ csize;
-    double *__restrict__ udeg;
-    int32_t *__restrict__ usize;
+    const double *__restrict__ cdeg;    // community degree at the start of the sweep
+    const int32_t *__restrict__ csize;  // community size at the start of the sweep
+    CommInfo *__restrict__ cupd;        // moves of this sweep (localCupdate)
     double *__restrict__ cw;
     double *__restrict__ frozen;
     const uint8_t *__restrict__ active; // nullptr when early termination is off
+    const int32_t *__restrict__ ref;     // reference id of each position (null: identity)
     double constant;
 };
 
@@ -67,15 +75,21 @@ __device__ __forceinline__ double gain_of(double eiy, double eix, double vd, dou
     return __dsub_rn(first, second);
 }
 
-// (gain, id) ordering of distGetMaxIndex: larger gain wins, equal gains go to the smaller id
+// (gain, id) ordering of distGetMaxIndex: larger gain wins, equal gains go to the
+// smaller reference id (looked up only on an exact tie)
 __device__ __forceinline__ bool better(bool ok_a, double g_a, int32_t c_a, bool ok_b, double g_b,
-                                       int32_t c_b) {
+                                       int32_t c_b, const int32_t *__restrict__ ref) {
     if (!ok_a) return false;
     if (!ok_b) return true;
-    return g_a > g_b || (g_a == g_b && c_a < c_b);
+    return g_a > g_b || (g_a == g_b && vg_rid(ref, c_a) < vg_rid(ref, c_b));
 }
 
 // decision + bookkeeping shared by all kernels (louvain.cpp:2275-2416)
+__device__ __forceinline__ void load_comm(const SweepArgs &a, int32_t c, double &deg, int32_t &size) {
+    deg = __ldg(a.cdeg + c);
+    size = __ldg(a.csize + c);
+}
+
 __device__ __forceinline__ void commit_vertex(const SweepArgs &a, int32_t v, int32_t cc,
                                               int32_t ccSize, double vd, bool has_edges,
                                               double counter0, bool ok, int32_t cand, int32_t csz) {
@@ -86,124 +100,115 @@ __device__ __forceinline__ void commit_vertex(const SweepArgs &a, int32_t v, int
             tgt = cand;
             maxSize = csz;
         }
-        if (maxSize == 1 && ccSize == 1 && tgt > cc) tgt = cc;
+        if (maxSize == 1 && ccSize == 1 && vg_rid(a.ref, tgt) > vg_rid(a.ref, cc)) tgt = cc;
     }
     const double cwv = has_edges ? counter0 : 0.0;
     a.cw[v] = cwv;
     if (a.active) a.frozen[v] = cwv;
     a.target[v] = tgt;
     if (tgt != cc) {
-        atomicAdd(&a.udeg[tgt], vd);
-        atomicAdd(&a.usize[tgt], 1);
-        atomicAdd(&a.udeg[cc], -vd);
-        atomicAdd(&a.usize[cc], -1);
+        atomicAdd(&a.cupd[tgt].deg, vd);
+        atomicAdd(&a.cupd[tgt].size, 1);
+        atomicAdd(&a.cupd[cc].deg, -vd);
+        atomicAdd(&a.cupd[cc].size, -1);
     }
 }
 
 // ---------------------------------------------------------------------------------
-// classes 0-3: G lanes per vertex, all edges in one chunk (degree <= G)
+// classes 0 and 1: one thread per vertex (degree <= T). All edge loads are issued
+// up front (streaming hint on the CSR, read-only path on the gathered arrays);
+// each community's counter is the reference's left fold in CSR order,
+// accumulated in an interleaved shared-memory slot of the community's first
+// occurrence. Candidate degrees are gathered eight at a time.
 
-template <int G>
-__global__ void __launch_bounds__(256) k_sweep_group(SweepArgs a, const int32_t *__restrict__ list,
-                                                     int64_t count) {
-    __shared__ double stage[256];
-    constexpr int GPW = 32 / G;
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int sub = lane & (G - 1);
-    const int grp = lane / G;
-    const unsigned gmask = (G == 32) ? full : (((1u << G) - 1u) << (grp * G));
-    double *my = stage + (threadIdx.x & ~31);
-    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = wg * GPW; base < count; base += nw * GPW) {
-        const int64_t idx = base + grp;
-        int32_t v = 0, cc = 0;
-        int64_t e0 = 0;
-        int d = 0;
-        bool run = false;
-        if (idx < count) {
-            v = list[idx];
-            e0 = a.rowptr[v];
-            d = (int)(a.rowptr[v + 1] - e0);
-            cc = a.curr[v];
-            run = true;
-            if (a.active && !a.active[v]) {
-                run = false;
-                if (sub == 0) a.cw[v] = a.frozen[v];
-            }
+template <bool LIST, int T, int NT>
+__global__ void __launch_bounds__(NT, (T <= 16 ? 3 : 3)) k_sweep_thread(
+    SweepArgs a, const int32_t *__restrict__ list, int64_t count) {
+    __shared__ double ssum[T][NT];
+    const int tid = threadIdx.x;
+    for (int64_t idx = blockIdx.x * (int64_t)NT + tid; idx < count; idx += (int64_t)gridDim.x * NT) {
+        const int32_t v = LIST ? list[idx] : (int32_t)idx;
+        const int64_t e0 = a.rowptr[v];
+        const int d = (int)(a.rowptr[v + 1] - e0);
+        if (!LIST && d > T) continue; // the list kernels take the larger degrees
+        if (a.active && !a.active[v]) {
+            a.cw[v] = a.frozen[v];
+            continue;
         }
-        const bool has = run && sub < d;
-        int32_t t = -1, c = -1;
-        double w = 0.0;
-        if (has) {
-            t = a.tail[e0 + sub];
-            w = a.weight[e0 + sub];
-            c = a.curr[t];
-        }
-        my[lane] = w;
-        const uint64_t key = has ? (((uint64_t)grp << 32) | (uint32_t)c)
-                                 : (0xFFFFFFFF00000000ULL | (uint64_t)lane);
-        const unsigned peers = __match_any_sync(full, key);
-        __syncwarp();
-        const int leader = __ffs(peers) - 1;
-        double sum = 0.0;
-        if (has && lane == leader) {
-            // counter of this community: weights folded in CSR order
-            unsigned m = peers & (peers - 1);
-            sum = my[leader];
-            while (m) {
-                const int b = __ffs(m) - 1;
-                sum = __dadd_rn(sum, my[b]);
-                m &= m - 1;
-            }
-        }
-        const unsigned selfm = __ballot_sync(full, has && t == v) & gmask;
+        const int32_t cc = __ldg(a.curr + v);
+        const double vd = a.vdeg[v];
+        const double ccDeg = __ldg(a.cdeg + cc);
+        int32_t c[T];
         double selfLoop = 0.0;
+        uint32_t first = 0; // bit j: edge j is the first occurrence of its community
         {
-            unsigned m = selfm;
-            while (m) {
-                const int b = __ffs(m) - 1;
-                selfLoop = __dadd_rn(selfLoop, my[b]);
-                m &= m - 1;
-            }
-        }
-        const unsigned ccm = __ballot_sync(full, has && c == cc) & gmask;
-        const double cnt0 = __shfl_sync(full, sum, ccm ? (__ffs(ccm) - 1) : lane);
-        const double counter0 = ccm ? cnt0 : 0.0;
-        double vd = 0.0, ccDeg = 0.0;
-        int32_t ccSize = 0;
-        if (run) {
-            vd = a.vdeg[v];
-            ccDeg = a.cdeg[cc];
-            ccSize = a.csize[cc];
-        }
-        double gain = 0.0;
-        int32_t cand = INT_MAX, csz = 0;
-        bool ok = false;
-        if (has && lane == leader && c != cc) {
-            const double ay = a.cdeg[c];
-            csz = a.csize[c];
-            gain = gain_of(sum, __dsub_rn(counter0, selfLoop), vd, ay, __dsub_rn(ccDeg, vd),
-                           a.constant);
-            ok = gain > 0.0;
-            cand = c;
-        }
+            double w[T];
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) {
-            const double og = __shfl_xor_sync(full, gain, o);
-            const int32_t oc = __shfl_xor_sync(full, cand, o);
-            const int32_t os = __shfl_xor_sync(full, csz, o);
-            const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
-            if (better(ook, og, oc, ok, gain, cand)) {
-                gain = og;
-                cand = oc;
-                csz = os;
-                ok = true;
+            for (int j = 0; j < T; j++) {
+                c[j] = -1;
+                w[j] = 0.0;
+                if (j < d) {
+                    const int32_t t = __ldcs(a.tail + e0 + j);
+                    w[j] = __ldcs(a.weight + e0 + j);
+                    c[j] = __ldg(a.curr + t);
+                    if (t == v) selfLoop = __dadd_rn(selfLoop, w[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < T; j++) {
+                if (j < d) {
+                    int fj = j;
+#pragma unroll
+                    for (int k = j - 1; k >= 0; k--)
+                        if (c[k] == c[j]) fj = k;
+                    if (fj == j) {
+                        first |= 1u << j;
+                        ssum[j][tid] = w[j];
+                    } else {
+                        ssum[fj][tid] = __dadd_rn(ssum[fj][tid], w[j]);
+                    }
+                }
             }
         }
-        if (run && sub == 0) commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, cand, csz);
-        __syncwarp();
+        double counter0 = 0.0;
+#pragma unroll
+        for (int j = 0; j < T; j++)
+            if (((first >> j) & 1u) && c[j] == cc) counter0 = ssum[j][tid];
+        const double eix = __dsub_rn(counter0, selfLoop);
+        const double ax = __dsub_rn(ccDeg, vd);
+        double bg = 0.0;
+        int32_t bc = INT_MAX;
+        bool ok = false;
+#pragma unroll
+        for (int b = 0; b < T; b += 8) {
+            double ay[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int j = b + q;
+                ay[q] = 0.0;
+                if (((first >> j) & 1u) && c[j] != cc) ay[q] = __ldg(a.cdeg + c[j]);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int j = b + q;
+                if (((first >> j) & 1u) && c[j] != cc) {
+                    const double g = gain_of(ssum[j][tid], eix, vd, ay[q], ax, a.constant);
+                    if (g > 0.0 && better(true, g, c[j], ok, bg, bc, a.ref)) {
+                        bg = g;
+                        bc = c[j];
+                        ok = true;
+                    }
+                }
+            }
+        }
+        // the singleton rule (louvain.cpp:2275-2276) needs the sizes only when
+        // the winner's id is larger than the current community's
+        int32_t ccSize = 0, bs = 0;
+        if (ok && vg_rid(a.ref, bc) > vg_rid(a.ref, cc)) {
+            ccSize = __ldg(a.csize + cc);
+            bs = __ldg(a.csize + bc);
+        }
+        commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, bc, bs);
     }
 }
 
@@ -313,8 +318,9 @@ __global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
             }
         }
         const double vd = a.vdeg[v];
-        const double ccDeg = a.cdeg[cc];
-        const int32_t ccSize = a.csize[cc];
+        double ccDeg;
+        int32_t ccSize;
+        load_comm(a, cc, ccDeg, ccSize);
         const double eix = __dsub_rn(counter0, selfLoop);
         const double ax = __dsub_rn(ccDeg, vd);
         double gain = 0.0;
@@ -323,11 +329,14 @@ __global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
         for (int s = lane; s < cap; s += 32) {
             const int32_t kk = keys[s];
             if (kk == EMPTY || kk == cc) continue;
-            const double g = gain_of(vals[s], eix, vd, a.cdeg[kk], ax, a.constant);
-            if (g > 0.0 && better(true, g, kk, ok, gain, cand)) {
+            double ay;
+            int32_t sz;
+            load_comm(a, kk, ay, sz);
+            const double g = gain_of(vals[s], eix, vd, ay, ax, a.constant);
+            if (g > 0.0 && better(true, g, kk, ok, gain, cand, a.ref)) {
                 gain = g;
                 cand = kk;
-                csz = a.csize[kk];
+                csz = sz;
                 ok = true;
             }
         }
@@ -337,7 +346,7 @@ __global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
             const int32_t oc = __shfl_xor_sync(full, cand, o);
             const int32_t os = __shfl_xor_sync(full, csz, o);
             const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
-            if (better(ook, og, oc, ok, gain, cand)) {
+            if (better(ook, og, oc, ok, gain, cand, a.ref)) {
                 gain = og;
                 cand = oc;
                 csz = os;
@@ -467,8 +476,9 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
         const double counter0 = sh.counter0;
         selfLoop = sh.self_part[0];
         const double vd = a.vdeg[v];
-        const double ccDeg = a.cdeg[cc];
-        const int32_t ccSize = a.csize[cc];
+        double ccDeg;
+        int32_t ccSize;
+        load_comm(a, cc, ccDeg, ccSize);
         const double eix = __dsub_rn(counter0, selfLoop);
         const double ax = __dsub_rn(ccDeg, vd);
         double gain = 0.0;
@@ -477,11 +487,14 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
         for (int64_t s = threadIdx.x; s < cap; s += CT_THREADS) {
             const int32_t kk = keys[s];
             if (kk == EMPTY || kk == cc) continue;
-            const double g = gain_of(vals[s], eix, vd, a.cdeg[kk], ax, a.constant);
-            if (g > 0.0 && better(true, g, kk, ok, gain, cand)) {
+            double ay;
+            int32_t sz;
+            load_comm(a, kk, ay, sz);
+            const double g = gain_of(vals[s], eix, vd, ay, ax, a.constant);
+            if (g > 0.0 && better(true, g, kk, ok, gain, cand, a.ref)) {
                 gain = g;
                 cand = kk;
-                csz = a.csize[kk];
+                csz = sz;
                 ok = true;
             }
         }
@@ -491,7 +504,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
             const int32_t oc = __shfl_xor_sync(full, cand, o);
             const int32_t os = __shfl_xor_sync(full, csz, o);
             const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
-            if (better(ook, og, oc, ok, gain, cand)) {
+            if (better(ook, og, oc, ok, gain, cand, a.ref)) {
                 gain = og;
                 cand = oc;
                 csz = os;
@@ -507,7 +520,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
         __syncthreads();
         if (threadIdx.x == 0) {
             for (int w = 1; w < CT_THREADS / 32; w++) {
-                if (better(sh.red_ok[w] != 0, sh.red_g[w], sh.red_c[w], ok, gain, cand)) {
+                if (better(sh.red_ok[w] != 0, sh.red_g[w], sh.red_c[w], ok, gain, cand, a.ref)) {
                     gain = sh.red_g[w];
                     cand = sh.red_c[w];
                     csz = sh.red_s[w];
@@ -537,8 +550,8 @@ __global__ void k_degree(const int64_t *__restrict__ rowptr, const double *__res
 
 // distInitLouvain (louvain.cpp:2138-2159) plus the early-termination buffers
 __global__ void k_init(int64_t nv, const double *__restrict__ vdeg, double *__restrict__ cdeg,
-                       int32_t *__restrict__ csize, double *__restrict__ udeg,
-                       int32_t *__restrict__ usize, int32_t *__restrict__ past,
+                       int32_t *__restrict__ csize, CommInfo *__restrict__ cupd,
+                       int32_t *__restrict__ past,
                        int32_t *__restrict__ curr, int32_t *__restrict__ target,
                        uint8_t *__restrict__ active, double *__restrict__ pcurr,
                        double *__restrict__ pprev) {
@@ -546,8 +559,11 @@ __global__ void k_init(int64_t nv, const double *__restrict__ vdeg, double *__re
          i += (int64_t)gridDim.x * blockDim.x) {
         cdeg[i] = vdeg[i];
         csize[i] = 1;
-        udeg[i] = 0.0;
-        usize[i] = 0;
+        CommInfo z;
+        z.deg = 0.0;
+        z.size = 0;
+        z.pad = 0;
+        cupd[i] = z;
         past[i] = (int32_t)i;
         curr[i] = (int32_t)i;
         target[i] = (int32_t)i;
@@ -579,22 +595,26 @@ constexpr int APPLY_THREADS = 512;
 // distUpdateLocalCinfo (louvain.cpp:2534-2547) fused with the two sums of
 // distComputeModularity (louvain.cpp:2496-2504) and the frozen-vertex count
 __global__ void __launch_bounds__(APPLY_THREADS) k_apply_mod(
-    int64_t nv, double *__restrict__ cdeg, int32_t *__restrict__ csize, double *__restrict__ udeg,
-    int32_t *__restrict__ usize, const double *__restrict__ cw, const uint8_t *__restrict__ active,
-    int do_sums, double *__restrict__ part) {
+    int64_t nv, double *__restrict__ cdeg, int32_t *__restrict__ csize, CommInfo *__restrict__ cupd,
+    const double *__restrict__ cw, const uint8_t *__restrict__ active, int do_sums,
+    double *__restrict__ part) {
     __shared__ double ws[32];
     double le = 0.0, la2 = 0.0, frozen = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const double du = udeg[i];
-        const int32_t ds = usize[i];
-        double cd = cdeg[i];
-        if (ds != 0 || du != 0.0) {
-            cd = __dadd_rn(cd, du);
+        const CommInfo u = cupd[i];
+        double cd;
+        if (u.size != 0 || u.deg != 0.0) {
+            cd = __dadd_rn(cdeg[i], u.deg);
             cdeg[i] = cd;
-            csize[i] += ds;
-            udeg[i] = 0.0;
-            usize[i] = 0;
+            csize[i] += u.size;
+            CommInfo z;
+            z.deg = 0.0;
+            z.size = 0;
+            z.pad = 0;
+            cupd[i] = z;
+        } else {
+            cd = do_sums ? cdeg[i] : 0.0;
         }
         if (do_sums) {
             le = __dadd_rn(le, cw[i]);
@@ -640,11 +660,11 @@ __global__ void k_mod_final(const double *__restrict__ part, int nblk, double co
 // `target == curr == past` compares the bool (target == curr) with past
 __global__ void k_swap_et13(int64_t nv, int numIters, int32_t *__restrict__ past,
                             int32_t *__restrict__ curr, int32_t *__restrict__ target,
-                            uint8_t *__restrict__ active) {
+                            uint8_t *__restrict__ active, const int32_t *__restrict__ ref) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t p = past[i], c = curr[i], t = target[i];
-        if (numIters > 2 && ((int32_t)(t == c) == p)) {
+        if (numIters > 2 && ((int32_t)(t == c) == vg_rid(ref, p))) {
             active[i] = 0;
         } else {
             past[i] = c;
@@ -697,27 +717,66 @@ __global__ void k_narrow(const int64_t *__restrict__ in, int64_t n, int64_t lim,
 }
 
 // bucket key of a vertex: (color bucket, degree class)
-__global__ void k_bucket_keys(const int64_t *__restrict__ rowptr, int64_t nv,
-                              const int32_t *__restrict__ colors, int64_t numColor,
-                              int32_t *__restrict__ key, int32_t *__restrict__ counts,
-                              unsigned long long *__restrict__ maxdeg) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t d = rowptr[i + 1] - rowptr[i];
-        int64_t cb = 0;
-        if (colors) cb = colors[i] < 0 ? numColor - 1 : colors[i];
-        const int32_t k = (int32_t)(cb * NCLS + degree_class(d));
-        key[i] = k;
-        atomicAdd(&counts[k], 1);
-        if (d > CT_MAXDEG) atomicMax(maxdeg, (unsigned long long)d);
-    }
+__device__ __forceinline__ int32_t bucket_key(const int64_t *__restrict__ rowptr, int64_t i,
+                                              const int32_t *__restrict__ colors, int64_t numColor,
+                                              int64_t *d_out) {
+    const int64_t d = rowptr[i + 1] - rowptr[i];
+    int64_t cb = 0;
+    if (colors) cb = colors[i] < 0 ? numColor - 1 : colors[i];
+    *d_out = d;
+    return (int32_t)(cb * NCLS + degree_class(d));
 }
 
-__global__ void k_bucket_scatter(int64_t nv, const int32_t *__restrict__ key,
-                                 int32_t *__restrict__ fill, int32_t *__restrict__ list) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
-         i += (int64_t)gridDim.x * blockDim.x)
-        list[atomicAdd(&fill[key[i]], 1)] = (int32_t)i;
+// Each block histograms a contiguous chunk of vertices in shared memory and
+// adds its counts to the global ones (one atomic per bucket per block).
+__global__ void k_bucket_count(const int64_t *__restrict__ rowptr, int64_t nv,
+                               const int32_t *__restrict__ colors, int64_t numColor, int nb,
+                               int64_t chunk, int32_t *__restrict__ counts,
+                               unsigned long long *__restrict__ maxdeg) {
+    extern __shared__ int32_t sc[];
+    __shared__ unsigned long long smax;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) sc[k] = 0;
+    if (threadIdx.x == 0) smax = 0;
+    __syncthreads();
+    const int64_t b0 = blockIdx.x * chunk, b1 = min(nv, b0 + chunk);
+    unsigned long long mx = 0;
+    for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        int64_t d;
+        const int32_t k = bucket_key(rowptr, i, colors, numColor, &d);
+        atomicAdd(&sc[k], 1);
+        if (d > CT_MAXDEG && (unsigned long long)d > mx) mx = (unsigned long long)d;
+    }
+    if (mx) atomicMax(&smax, mx);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nb; k += blockDim.x)
+        if (sc[k]) atomicAdd(&counts[k], sc[k]);
+    if (threadIdx.x == 0 && smax) atomicMax(maxdeg, smax);
+}
+
+// Each block reserves a range per bucket with one atomic and places its vertices
+// there (order inside a bucket follows the blocks' chunks).
+__global__ void k_bucket_place(const int64_t *__restrict__ rowptr, int64_t nv,
+                               const int32_t *__restrict__ colors, int64_t numColor, int nb,
+                               int64_t chunk, int32_t *__restrict__ fill,
+                               int32_t *__restrict__ list) {
+    extern __shared__ int32_t sc[]; // [0, nb) counts then local cursors, [nb, 2nb) bases
+    int32_t *base = sc + nb;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) sc[k] = 0;
+    __syncthreads();
+    const int64_t b0 = blockIdx.x * chunk, b1 = min(nv, b0 + chunk);
+    int64_t d;
+    for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x)
+        atomicAdd(&sc[bucket_key(rowptr, i, colors, numColor, &d)], 1);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        base[k] = sc[k] ? atomicAdd(&fill[k], sc[k]) : 0;
+        sc[k] = 0;
+    }
+    __syncthreads();
+    for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        const int32_t k = bucket_key(rowptr, i, colors, numColor, &d);
+        list[base[k] + atomicAdd(&sc[k], 1)] = (int32_t)i;
+    }
 }
 
 } // namespace
@@ -736,16 +795,18 @@ static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors,
                           Buckets &b) {
     const int64_t nv = g->nv;
     const int64_t nb = numColor * NCLS;
+    VG_REQUIRE(nb <= 6000, "too many color buckets (%lld colors)", (long long)numColor);
     b.ncolor = numColor;
-    DevBuf<int32_t> key(ctx, nv);
     DevBuf<int32_t> counts(ctx, nb);
     DevBuf<unsigned long long> maxdeg(ctx, 1);
     VG_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int32_t) * nb, ctx->stream));
     VG_CUDA(cudaMemsetAsync(maxdeg.p, 0, sizeof(unsigned long long), ctx->stream));
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nv + 1023) / 1024, 4LL * ctx->sm_count));
+    const int64_t chunk = (nv + blocks - 1) / blocks;
     if (nv) {
         LaunchTimer lt(ctx);
-        k_bucket_keys<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(
-            g->rowptr, nv, colors, numColor, key.p, counts.p, maxdeg.p);
+        k_bucket_count<<<blocks, 256, sizeof(int32_t) * nb, ctx->stream>>>(
+            g->rowptr, nv, colors, numColor, (int)nb, chunk, counts.p, maxdeg.p);
     }
     VG_CHECK_LAUNCH();
     std::vector<int32_t> hc(nb);
@@ -766,8 +827,8 @@ static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors,
     b.list.alloc(ctx, nv);
     if (nv) {
         LaunchTimer lt(ctx);
-        k_bucket_scatter<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(nv, key.p, counts.p,
-                                                                          b.list.p);
+        k_bucket_place<<<blocks, 256, 2 * sizeof(int32_t) * nb, ctx->stream>>>(
+            g->rowptr, nv, colors, numColor, (int)nb, chunk, counts.p, b.list.p);
     }
     VG_CHECK_LAUNCH();
     vg_sync(ctx); // keep `fill` alive until the copy is done
@@ -796,25 +857,35 @@ struct GlobalTable {
     int blocks = 0;
 };
 
-// launch the sweep kernels over the lists of one color bucket
+// launch the sweep kernels over one color bucket; with `natural` the low-degree
+// class runs over all vertices in id order instead of its list
 static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64_t color,
-                        GlobalTable &gt) {
+                        GlobalTable &gt, bool natural, int64_t nv) {
     const int32_t *list = b.list.p;
     for (int cls = 0; cls < NCLS; cls++) {
         const int64_t s = b.start[color * NCLS + cls], e = b.start[color * NCLS + cls + 1];
         const int64_t n = e - s;
+        if (cls == 0 && natural) {
+            if (nv == 0) continue;
+            LaunchTimer lt(ctx);
+            k_sweep_thread<false, TMAX, TB><<<vg_grid(ctx, nv, TB, 8), TB, 0, ctx->stream>>>(a, nullptr, nv);
+            VG_CHECK_LAUNCH();
+            continue;
+        }
         if (n == 0) continue;
         LaunchTimer lt(ctx);
         switch (cls) {
-        case 0: k_sweep_group<4><<<vg_grid(ctx, n * 4, 256, 8), 256, 0, ctx->stream>>>(a, list + s, n); break;
-        case 1: k_sweep_group<8><<<vg_grid(ctx, n * 8, 256, 8), 256, 0, ctx->stream>>>(a, list + s, n); break;
-        case 2: k_sweep_group<16><<<vg_grid(ctx, n * 16, 256, 8), 256, 0, ctx->stream>>>(a, list + s, n); break;
-        case 3: k_sweep_group<32><<<vg_grid(ctx, n * 32, 256, 8), 256, 0, ctx->stream>>>(a, list + s, n); break;
-        case 4:
+        case 0:
+            k_sweep_thread<true, TMAX, TB><<<vg_grid(ctx, n, TB, 8), TB, 0, ctx->stream>>>(a, list + s, n);
+            break;
+        case 1:
+            k_sweep_thread<true, 32, 128><<<vg_grid(ctx, n, 128, 12), 128, 0, ctx->stream>>>(a, list + s, n);
+            break;
+        case 2:
             k_sweep_warp<<<vg_grid(ctx, n * 32, WT_WARPS * 32, 4), WT_WARPS * 32, warp_smem_bytes(),
                            ctx->stream>>>(a, list + s, n);
             break;
-        case 5:
+        case 3:
             k_sweep_cta<false><<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, 2), CT_THREADS,
                                  cta_smem_bytes(), ctx->stream>>>(a, list + s, n, nullptr, nullptr, 0);
             break;
@@ -853,8 +924,10 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         }
     }
     const bool use_et = et != 0;
-    DevBuf<double> vdeg(ctx, nv), cdeg(ctx, nv), udeg(ctx, nv), cw(ctx, nv);
-    DevBuf<int32_t> csize(ctx, nv), usize(ctx, nv);
+    DevBuf<double> vdeg(ctx, nv), cw(ctx, nv);
+    DevBuf<double> cdeg(ctx, nv);
+    DevBuf<int32_t> csize(ctx, nv);
+    DevBuf<CommInfo> cupd(ctx, nv);
     DevBuf<int32_t> A(ctx, nv), B(ctx, nv), C(ctx, nv);
     DevBuf<double> frozen, pA, pB;
     DevBuf<uint8_t> active;
@@ -878,7 +951,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
     const double constant = 1.0 / twice_m; // distCalcConstantForSecondTerm (louvain.cpp:2217)
     if (nv) {
         LaunchTimer lt(ctx);
-        k_init<<<grid, 256, 0, ctx->stream>>>(nv, vdeg.p, cdeg.p, csize.p, udeg.p, usize.p, A.p, B.p,
+        k_init<<<grid, 256, 0, ctx->stream>>>(nv, vdeg.p, cdeg.p, csize.p, cupd.p, A.p, B.p,
                                               C.p, active.p, pA.p, pB.p);
     }
     VG_CHECK_LAUNCH();
@@ -889,7 +962,8 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         int64_t cap = 32;
         while (cap < 2 * bk.maxdeg_global) cap <<= 1;
         int64_t n6 = 0;
-        for (int64_t c = 0; c < numColor; c++) n6 = std::max(n6, bk.start[c * NCLS + 7] - bk.start[c * NCLS + 6]);
+        for (int64_t c = 0; c < numColor; c++)
+            n6 = std::max(n6, bk.start[c * NCLS + 5] - bk.start[c * NCLS + 4]);
         gt.blocks = (int)std::min<int64_t>(n6, (int64_t)ctx->sm_count * 2);
         gt.cap = cap;
         gt.keys.alloc(ctx, (size_t)cap * gt.blocks);
@@ -920,19 +994,19 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         a.vdeg = vdeg.p;
         a.cdeg = cdeg.p;
         a.csize = csize.p;
-        a.udeg = udeg.p;
-        a.usize = usize.p;
+        a.cupd = cupd.p;
         a.cw = cw.p;
         a.frozen = frozen.p;
         a.active = use_et ? active.p : nullptr;
+        a.ref = g->ref;
         a.constant = constant;
         if (timing) VG_CUDA(cudaEventRecord(ev0, ctx->stream));
         for (int64_t ci = 0; ci < numColor; ci++) {
-            sweep_color(ctx, a, bk, ci, gt);
+            sweep_color(ctx, a, bk, ci, gt, ordering == 0, nv);
             if (ordering == 1 && nv) { // per-color community update (louvain.cpp:724-735)
                 LaunchTimer lt(ctx);
                 k_apply_mod<<<APPLY_BLOCKS, APPLY_THREADS, 0, ctx->stream>>>(
-                    nv, cdeg.p, csize.p, udeg.p, usize.p, cw.p, a.active, 0, part.p);
+                    nv, cdeg.p, csize.p, cupd.p, cw.p, a.active, 0, part.p);
                 VG_CHECK_LAUNCH();
             }
         }
@@ -941,7 +1015,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
             {
                 LaunchTimer lt(ctx);
                 k_apply_mod<<<APPLY_BLOCKS, APPLY_THREADS, 0, ctx->stream>>>(
-                    nv, cdeg.p, csize.p, udeg.p, usize.p, cw.p, a.active, 1, part.p);
+                    nv, cdeg.p, csize.p, cupd.p, cw.p, a.active, 1, part.p);
             }
             VG_CHECK_LAUNCH();
             {
@@ -979,7 +1053,8 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
             target = tmp;
         } else if (et == 1 || et == 3) {
             LaunchTimer lt(ctx);
-            k_swap_et13<<<grid, 256, 0, ctx->stream>>>(nv, numIters, past, curr, target, active.p);
+            k_swap_et13<<<grid, 256, 0, ctx->stream>>>(nv, numIters, past, curr, target, active.p,
+                                                       g->ref);
             VG_CHECK_LAUNCH();
         } else {
             {
@@ -1048,7 +1123,7 @@ extern "C" vg_status vg_louvain_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_p
     return vg_guard(ctx, [&] {
         VG_CUDA(cudaSetDevice(ctx->device));
         run_phase(ctx, g, p, mod_out, iters_out, nullptr);
-        if (cvect_out) vg_download_comm(ctx, g->comm, g->nv, cvect_out);
+        if (cvect_out) vg_download_comm_ref(ctx, g, g->comm, cvect_out);
     });
 }
 

@@ -336,8 +336,8 @@ __global__ void k_run_heads(const uint64_t *__restrict__ keys, int64_t m, bool c
 __global__ void k_fold_runs(const uint64_t *__restrict__ keys, const uint32_t *__restrict__ order,
                             const double *__restrict__ w, const int32_t *__restrict__ head,
                             const int64_t *__restrict__ pos, int64_t m, int b2,
-                            int32_t *__restrict__ out_tail, double *__restrict__ out_w,
-                            int64_t *__restrict__ rowcount) {
+                            const int32_t *__restrict__ dst_map, int32_t *__restrict__ out_tail,
+                            double *__restrict__ out_w, int64_t *__restrict__ rowcount) {
     const uint64_t mask = (b2 >= 64) ? ~0ULL : ((1ULL << b2) - 1ULL);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -350,7 +350,8 @@ __global__ void k_fold_runs(const uint64_t *__restrict__ keys, const uint32_t *_
             j++;
         }
         const int64_t o = pos[i];
-        out_tail[o] = (int32_t)(k & mask);
+        const int32_t lo = (int32_t)(k & mask);
+        out_tail[o] = dst_map ? dst_map[lo] : lo;
         out_w[o] = s;
         atomicAdd((unsigned long long *)&rowcount[k >> b2], 1ULL);
     }
@@ -365,7 +366,7 @@ static int bits_for(int64_t n) {
 }
 
 vg_graph *vg_csr_from_triples(vg_ctx *ctx, int64_t nv, DevBuf<int32_t> &src, DevBuf<int32_t> &dst,
-                              DevBuf<double> &w, int64_t m, bool combine) {
+                              DevBuf<double> &w, int64_t m, bool combine, const int32_t *dst_map) {
     const int b2 = bits_for(nv > 1 ? nv : 2);
     VG_REQUIRE(2 * b2 <= 64, "graph too large for 64-bit sort keys");
     VG_REQUIRE(m < (int64_t)UINT32_MAX, "too many edges for one sort (%lld)", (long long)m);
@@ -401,7 +402,7 @@ vg_graph *vg_csr_from_triples(vg_ctx *ctx, int64_t nv, DevBuf<int32_t> &src, Dev
         {
             LaunchTimer lt(ctx);
             k_fold_runs<<<vg_grid(ctx, m, 256), 256, 0, ctx->stream>>>(
-                keys.p, order.p, w.p, head.p, pos.p, m, b2, tail.p, weight.p, rowptr.p);
+                keys.p, order.p, w.p, head.p, pos.p, m, b2, dst_map, tail.p, weight.p, rowptr.p);
         }
         VG_CHECK_LAUNCH();
     }

@@ -67,36 +67,180 @@ __global__ void k_triples(const int64_t *__restrict__ rowptr, const int32_t *__r
 
 } // namespace
 
+// Graph in the library's layout: communities are named by positions. The next
+// level's reference numbering is the first appearance in REFERENCE vertex order
+// (min reference id of the members); its positions follow the first member's
+// position, so the coarse graph keeps the locality of the fine one. Triples are
+// emitted in reference vertex order, so equal pairs fold in the reference's order.
+namespace {
+
+__global__ void k_first_ref(const int32_t *__restrict__ comm, int64_t nv,
+                            const int32_t *__restrict__ ref, int32_t *__restrict__ first) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nv;
+         p += (int64_t)gridDim.x * blockDim.x)
+        atomicMin(&first[comm[p]], ref[p]);
+}
+
+// flag_ref[r] = 1 where r is the first (smallest-reference-id) member of its
+// community; flag_pos[p] likewise by position
+__global__ void k_first_flags(const int32_t *__restrict__ comm, int64_t nv,
+                              const int32_t *__restrict__ ref, const int32_t *__restrict__ first_ref,
+                              const int32_t *__restrict__ first_pos, int32_t *__restrict__ flag_ref,
+                              int32_t *__restrict__ flag_pos) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nv;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t c = comm[p];
+        flag_ref[ref[p]] = first_ref[c] == ref[p] ? 1 : 0;
+        flag_pos[p] = first_pos[c] == (int32_t)p ? 1 : 0;
+    }
+}
+
+__global__ void k_new_ids(const int32_t *__restrict__ comm, int64_t nv,
+                          const int32_t *__restrict__ first_ref, const int64_t *__restrict__ rank_ref,
+                          const int32_t *__restrict__ first_pos, const int64_t *__restrict__ rank_pos,
+                          int32_t *__restrict__ new_ref, int32_t *__restrict__ new_pos,
+                          int32_t *__restrict__ next_ref, int32_t *__restrict__ next_pos) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nv;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t c = comm[p];
+        const int32_t nr = (int32_t)rank_ref[first_ref[c]];
+        const int32_t np = (int32_t)rank_pos[first_pos[c]];
+        new_ref[p] = nr;
+        new_pos[p] = np;
+        if (first_pos[c] == (int32_t)p) {
+            next_ref[np] = nr;
+            next_pos[nr] = np;
+        }
+    }
+}
+
+// degree of each vertex in reference order
+__global__ void k_deg_by_ref(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ pos,
+                             int64_t nv, int64_t *__restrict__ deg) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nv;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t p = pos[r];
+        deg[r] = rowptr[p + 1] - rowptr[p];
+    }
+}
+
+// triples in reference vertex order, CSR order inside a row
+__global__ void k_triples_ref(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
+                              const double *__restrict__ w, int64_t nv,
+                              const int32_t *__restrict__ pos, const int64_t *__restrict__ off,
+                              const int32_t *__restrict__ new_pos, const int32_t *__restrict__ new_ref,
+                              int32_t *__restrict__ src, int32_t *__restrict__ dst,
+                              double *__restrict__ wo) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = wg; r < nv; r += nw) {
+        const int32_t p = pos[r];
+        const int32_t s = new_pos[p];
+        const int64_t e0 = rowptr[p], len = rowptr[p + 1] - e0, o = off[r];
+        for (int64_t j = lane; j < len; j += 32) {
+            src[o + j] = s;
+            dst[o + j] = new_ref[tail[e0 + j]];
+            wo[o + j] = w[e0 + j];
+        }
+    }
+}
+
+} // namespace
+
 vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm) {
     const int64_t nv = g->nv, ne = g->ne;
-    DevBuf<int32_t> first(ctx, nv), flag(ctx, nv), newof(ctx, nv);
-    DevBuf<int64_t> rank(ctx, nv);
     const int grid = vg_grid(ctx, nv, 256);
+    if (!g->ref) {
+        // reference layout: first appearance by position is first appearance by id
+        DevBuf<int32_t> first(ctx, nv), flag(ctx, nv), newof(ctx, nv);
+        DevBuf<int64_t> rank(ctx, nv);
+        int64_t nc = 0;
+        if (nv) {
+            { LaunchTimer lt(ctx); k_fill_first<<<grid, 256, 0, ctx->stream>>>(first.p, nv); }
+            VG_CHECK_LAUNCH();
+            { LaunchTimer lt(ctx); k_first_member<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p); }
+            VG_CHECK_LAUNCH();
+            { LaunchTimer lt(ctx); k_first_flag<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p, flag.p); }
+            VG_CHECK_LAUNCH();
+            nc = vg_exclusive_scan_i32_to_i64(ctx, flag.p, rank.p, nv);
+            { LaunchTimer lt(ctx); k_new_of<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p, rank.p, newof.p); }
+            VG_CHECK_LAUNCH();
+        }
+        first.release();
+        flag.release();
+        rank.release();
+        DevBuf<int32_t> src(ctx, ne), dst(ctx, ne);
+        DevBuf<double> w(ctx, ne);
+        if (ne) {
+            LaunchTimer lt(ctx);
+            k_triples<<<vg_grid(ctx, nv * 32, 256), 256, 0, ctx->stream>>>(
+                g->rowptr, g->tail, g->weight, nv, newof.p, src.p, dst.p, w.p);
+        }
+        VG_CHECK_LAUNCH();
+        newof.release();
+        return vg_csr_from_triples(ctx, nc, src, dst, w, ne, true);
+    }
+    DevBuf<int32_t> first_ref(ctx, nv), first_pos(ctx, nv), flag_ref(ctx, nv), flag_pos(ctx, nv);
+    DevBuf<int64_t> rank_ref(ctx, nv), rank_pos(ctx, nv);
+    DevBuf<int32_t> new_ref(ctx, nv), new_pos(ctx, nv), next_ref(ctx, nv), next_pos(ctx, nv);
     int64_t nc = 0;
     if (nv) {
-        { LaunchTimer lt(ctx); k_fill_first<<<grid, 256, 0, ctx->stream>>>(first.p, nv); }
+        { LaunchTimer lt(ctx); k_fill_first<<<grid, 256, 0, ctx->stream>>>(first_ref.p, nv); }
         VG_CHECK_LAUNCH();
-        { LaunchTimer lt(ctx); k_first_member<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p); }
+        { LaunchTimer lt(ctx); k_fill_first<<<grid, 256, 0, ctx->stream>>>(first_pos.p, nv); }
         VG_CHECK_LAUNCH();
-        { LaunchTimer lt(ctx); k_first_flag<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p, flag.p); }
+        { LaunchTimer lt(ctx); k_first_ref<<<grid, 256, 0, ctx->stream>>>(comm, nv, g->ref, first_ref.p); }
         VG_CHECK_LAUNCH();
-        nc = vg_exclusive_scan_i32_to_i64(ctx, flag.p, rank.p, nv);
-        { LaunchTimer lt(ctx); k_new_of<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p, rank.p, newof.p); }
+        { LaunchTimer lt(ctx); k_first_member<<<grid, 256, 0, ctx->stream>>>(comm, nv, first_pos.p); }
+        VG_CHECK_LAUNCH();
+        { LaunchTimer lt(ctx);
+          k_first_flags<<<grid, 256, 0, ctx->stream>>>(comm, nv, g->ref, first_ref.p, first_pos.p,
+                                                       flag_ref.p, flag_pos.p); }
+        VG_CHECK_LAUNCH();
+        nc = vg_exclusive_scan_i32_to_i64(ctx, flag_ref.p, rank_ref.p, nv);
+        vg_exclusive_scan_i32_to_i64(ctx, flag_pos.p, rank_pos.p, nv);
+        { LaunchTimer lt(ctx);
+          k_new_ids<<<grid, 256, 0, ctx->stream>>>(comm, nv, first_ref.p, rank_ref.p, first_pos.p,
+                                                   rank_pos.p, new_ref.p, new_pos.p, next_ref.p,
+                                                   next_pos.p); }
         VG_CHECK_LAUNCH();
     }
-    first.release();
-    flag.release();
-    rank.release();
+    flag_ref.release();
+    flag_pos.release();
+    rank_ref.release();
+    rank_pos.release();
+    first_ref.release();
+    first_pos.release();
+    DevBuf<int64_t> off(ctx, nv + 1);
+    VG_CUDA(cudaMemsetAsync(off.p + nv, 0, sizeof(int64_t), ctx->stream));
+    if (nv) {
+        LaunchTimer lt(ctx);
+        k_deg_by_ref<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->pos, nv, off.p);
+    }
+    VG_CHECK_LAUNCH();
+    vg_exclusive_scan_i64(ctx, off.p, nv + 1);
     DevBuf<int32_t> src(ctx, ne), dst(ctx, ne);
     DevBuf<double> w(ctx, ne);
     if (ne) {
         LaunchTimer lt(ctx);
-        k_triples<<<vg_grid(ctx, nv * 32, 256), 256, 0, ctx->stream>>>(g->rowptr, g->tail, g->weight,
-                                                                      nv, newof.p, src.p, dst.p, w.p);
+        k_triples_ref<<<vg_grid(ctx, nv * 32, 256), 256, 0, ctx->stream>>>(
+            g->rowptr, g->tail, g->weight, nv, g->pos, off.p, new_pos.p, new_ref.p, src.p, dst.p, w.p);
     }
     VG_CHECK_LAUNCH();
-    newof.release();
-    return vg_csr_from_triples(ctx, nc, src, dst, w, ne, true);
+    off.release();
+    new_ref.release();
+    new_pos.release();
+    vg_graph *h = vg_csr_from_triples(ctx, nc, src, dst, w, ne, true, next_pos.p);
+    // the arrays were sized nv; the next level keeps its first nc entries
+    DevBuf<int32_t> r2(ctx, nc), p2(ctx, nc);
+    if (nc) {
+        VG_CUDA(cudaMemcpyAsync(r2.p, next_ref.p, sizeof(int32_t) * nc, cudaMemcpyDeviceToDevice, ctx->stream));
+        VG_CUDA(cudaMemcpyAsync(p2.p, next_pos.p, sizeof(int32_t) * nc, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    h->ref = r2.detach();
+    h->pos = p2.detach();
+    return h;
 }
 
 extern "C" vg_status vg_rebuild(vg_ctx *ctx, vg_graph *g, const int64_t *cvect) {
@@ -108,6 +252,7 @@ extern "C" vg_status vg_rebuild(vg_ctx *ctx, vg_graph *g, const int64_t *cvect) 
         if (cvect) {
             up.alloc(ctx, g->nv);
             vg_upload_ids(ctx, cvect, g->nv, g->nv, up.p);
+            vg_ref_to_pos_inplace(ctx, g, up.p, true);
             comm = up.p;
         }
         VG_REQUIRE(comm != nullptr || g->nv == 0, "vg_rebuild: no communities (run a phase first)");

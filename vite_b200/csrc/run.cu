@@ -12,7 +12,6 @@ void vg_phase_internal(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, doubl
 int64_t vg_color_internal(vg_ctx *ctx, vg_graph *g, int64_t nHash, int32_t target_percent,
                           int32_t single_iteration);
 vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm);
-void vg_download_comm(vg_ctx *ctx, const int32_t *comm, int64_t n, int64_t *out);
 
 namespace {
 
@@ -77,6 +76,16 @@ extern "C" vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g0, const vg_ru
         view.comm = nullptr;
         view.num_colors = -1;
         vg_graph *cur = &view;
+        VG_REQUIRE(rp->layout >= 0 && rp->layout <= 2, "layout must be 0, 1 or 2");
+        double layout_s = 0.0;
+        if (!g0->ref && (rp->layout == 1 || (rp->layout == 2 && g0->nv >= (1 << 18)))) {
+            EventTimer tl(ctx->stream);
+            DevBuf<int32_t> order;
+            vg_bfs_order(ctx, g0, order);
+            owned = vg_apply_layout(ctx, g0, order.p);
+            cur = owned;
+            layout_s = tl.stop_ms() * 1e-3;
+        }
         std::vector<int64_t> commAll;
         if (comm_out) commAll.assign(g0->nv, -1);
         double currMod = -1.0, prevMod = -1.0, threshold = rp->threshold;
@@ -100,6 +109,7 @@ extern "C" vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g0, const vg_ru
                 vg_level_stat ls = {};
                 ls.nv = cur->nv;
                 ls.ne = cur->ne;
+                if (phase == 0) ls.seconds_layout = layout_s;
                 vg_phase_params pp = {};
                 pp.lower = currMod;
                 pp.threshold = threshold;
@@ -128,7 +138,7 @@ extern "C" vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g0, const vg_ru
                 if (accepted) {
                     if (comm_out) {
                         std::vector<int64_t> cv(cur->nv);
-                        vg_download_comm(ctx, cur->comm, cur->nv, cv.data());
+                        vg_download_comm_ref(ctx, cur, cur->comm, cv.data());
                         compose_output(commAll, cv, phase);
                     }
                     if (!rp->one_phase) {

@@ -121,9 +121,26 @@ struct vg_graph {
     // coloring attached by vg_color / vg_set_colors (int32, -1 uncolored)
     int32_t *colors = nullptr;
     int64_t num_colors = -1;   // reference's nextColor; -1 = none
-    // communities of the last phase (int32), kept for vg_rebuild
+    // communities of the last phase (int32, positions), kept for vg_rebuild
     int32_t *comm = nullptr;
+    // HBM layout: position p holds the vertex with reference id ref[p]; pos is the
+    // inverse. Both null when positions are the reference ids.
+    int32_t *ref = nullptr;
+    int32_t *pos = nullptr;
 };
+
+// reference id of the vertex (or community) at position p
+__device__ __forceinline__ int32_t vg_rid(const int32_t *__restrict__ ref, int32_t p) {
+    return ref ? __ldg(ref + p) : p;
+}
+
+// layout helpers (layout.cu)
+void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order);
+vg_graph *vg_apply_layout(vg_ctx *ctx, const vg_graph *g, const int32_t *order);
+vg_graph *vg_remove_layout(vg_ctx *ctx, const vg_graph *g);
+void vg_download_comm_ref(vg_ctx *ctx, const vg_graph *g, const int32_t *comm, int64_t *out);
+void vg_download_vals_ref(vg_ctx *ctx, const vg_graph *g, const int32_t *x, int64_t *out);
+void vg_ref_to_pos_inplace(vg_ctx *ctx, const vg_graph *g, int32_t *x, bool are_ids);
 
 void vg_graph_release(vg_ctx *ctx, vg_graph *g);
 // the graph takes ownership of the three arrays
@@ -143,9 +160,11 @@ double vg_sum_f64(vg_ctx *ctx, const double *x, int64_t n);
 
 // CSR from (src, dst, w) triples in their given order: stable sort by (src, dst),
 // adjacent duplicates combined by summing their weights in order when `combine`.
-// nv rows; the three inputs are consumed (freed).
+// nv rows; the three inputs are consumed (freed). With dst_map the stored tail
+// is dst_map[dst] (dst orders the row, dst_map names the position).
 vg_graph *vg_csr_from_triples(vg_ctx *ctx, int64_t nv, DevBuf<int32_t> &src,
-                              DevBuf<int32_t> &dst, DevBuf<double> &w, int64_t m, bool combine);
+                              DevBuf<int32_t> &dst, DevBuf<double> &w, int64_t m, bool combine,
+                              const int32_t *dst_map = nullptr);
 
 // ---------------------------------------------------------------------------------
 // kernels shared across files
