@@ -98,6 +98,11 @@ size_t vg_ctx_bytes_in_use(const vg_ctx *ctx);
  * enabled, the sum of their device times in ms (events around each launch). */
 vg_status vg_ctx_profile(vg_ctx *ctx, int32_t enable, double *kernel_ms_out,
                          int64_t *launches_out, int32_t reset);
+/* Grow the context's device memory pool to at least `bytes` now (no reference
+ * counterpart). Freed memory stays in the pool, so later phases and rebuilds of
+ * up to this working set allocate without mapping new memory mid-run. Counted
+ * against the budget only while held (it is released back to the pool at once). */
+vg_status vg_ctx_reserve(vg_ctx *ctx, size_t bytes);
 /* The CUDA stream (cudaStream_t) all of the context's work runs on, so callers
  * can time it with events or order their own work after it. */
 vg_status vg_ctx_stream(vg_ctx *ctx, void **stream_out);

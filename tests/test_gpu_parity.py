@@ -248,6 +248,28 @@ def test_rebuild_matches_oracle(ctx, maker):
     assert_graph_equal(g.download(), vo.rebuild(gref, cv))
 
 
+@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("case", ["one_community", "blocks_of_600", "random_blocks"])
+def test_rebuild_segment_classes(ctx, case, layout):
+    """Next-level segments of every size class: warp (<=1024 entries), CTA (<=8192) and
+    the single-CTA global radix path (above), with real weights folded in order."""
+    if case == "one_community":
+        gref = vo.reweight(star_graph(9000), 2, 5)
+        cv = np.full(gref.nv, 17, np.int64)
+    elif case == "blocks_of_600":
+        gref = vo.rgg(65536)
+        cv = (np.arange(gref.nv) // 600 * 600).astype(np.int64)
+    else:
+        gref = vo.reweight(vo.ba(30000, 8, 4), 2, 9)
+        rng = np.random.default_rng(3)
+        cv = rng.integers(0, 40, gref.nv).astype(np.int64) * 7
+    g = upload(ctx, gref)
+    if layout:
+        ctx.reorder(g, 1)
+    ctx.rebuild(g, cv)
+    assert_graph_equal(g.download(), vo.rebuild(gref, cv))
+
+
 def test_run_matches_oracle_run(ctx, golden):
     e = golden["ba4k_c8_t2"]
     gref = vo.golden_graph(e)

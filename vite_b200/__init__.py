@@ -30,7 +30,7 @@ _STATUS_NAMES = {0: "VG_OK", 1: "VG_ERR_ARG", 2: "VG_ERR_OOM", 3: "VG_ERR_CUDA",
 
 EXPORTED_SYMBOLS = [
     "vg_ctx_create", "vg_ctx_destroy", "vg_last_error", "vg_ctx_bytes_in_use", "vg_ctx_profile",
-    "vg_ctx_stream",
+    "vg_ctx_stream", "vg_ctx_reserve",
     "vg_graph_upload", "vg_graph_info", "vg_graph_download", "vg_graph_free", "vg_vertex_degree",
     "vg_louvain_phase", "vg_color", "vg_set_colors", "vg_rebuild", "vg_louvain_run",
     "vg_generate_rgg", "vg_generate_ba", "vg_generate_er", "vg_graph_reweight",
@@ -94,6 +94,7 @@ def lib() -> C.CDLL:
         L.vg_ctx_bytes_in_use.restype = C.c_size_t
         L.vg_ctx_profile.argtypes = [vp, C.c_int32, _f64p, _i64p, C.c_int32]
         L.vg_ctx_stream.argtypes = [vp, C.POINTER(vp)]
+        L.vg_ctx_reserve.argtypes = [vp, C.c_size_t]
         L.vg_graph_upload.argtypes = [vp, C.c_int64, C.c_int64, _i64p, vp, C.POINTER(vp)]
         L.vg_graph_info.argtypes = [vp, _i64p, _i64p]
         L.vg_graph_download.argtypes = [vp, vp, _i64p, vp]
@@ -204,6 +205,10 @@ class Context:
     @property
     def bytes_in_use(self) -> int:
         return int(lib().vg_ctx_bytes_in_use(self.handle))
+
+    def reserve(self, nbytes: int) -> None:
+        """Pre-grow the device memory pool (no mid-run mapping up to this working set)."""
+        self._check(lib().vg_ctx_reserve(self.handle, int(nbytes)))
 
     @property
     def stream(self) -> int:

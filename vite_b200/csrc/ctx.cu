@@ -132,6 +132,16 @@ extern "C" vg_status vg_ctx_destroy(vg_ctx *ctx) {
     return VG_OK;
 }
 
+extern "C" vg_status vg_ctx_reserve(vg_ctx *ctx, size_t bytes) {
+    if (!ctx) return VG_ERR_ARG;
+    return vg_guard(ctx, [&] {
+        VG_CUDA(cudaSetDevice(ctx->device));
+        void *p = vg_alloc(ctx, bytes);
+        vg_free(ctx, p, bytes);
+        vg_sync(ctx);
+    });
+}
+
 extern "C" vg_status vg_ctx_stream(vg_ctx *ctx, void **stream_out) {
     if (!ctx || !stream_out) return VG_ERR_ARG;
     *stream_out = (void *)ctx->stream;

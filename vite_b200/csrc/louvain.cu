@@ -64,6 +64,7 @@ struct SweepArgs {
     double *__restrict__ frozen;
     const uint8_t *__restrict__ active; // nullptr when early termination is off
     const int32_t *__restrict__ ref;     // reference id of each position (null: identity)
+    int64_t ne;                          // CSR entries (bounds of the vector loads)
     double constant;
 };
 
@@ -209,6 +210,156 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? 3 : 3)) k_sweep_thread(
             bs = __ldg(a.csize + bc);
         }
         commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, bc, bs);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// class 0 in vertex order: a warp takes 32 consecutive vertices, whose rows form
+// one contiguous edge range, and stages that range into shared memory with
+// coalesced 128-bit loads; each lane then works on its own vertex from shared
+// memory. Counters fold in place, in the staged weights of the lane's row, in
+// CSR order (slot of the community's first occurrence). A range longer than the
+// staging buffer falls back to per-lane copies of the (short) rows.
+
+constexpr int TILE_CAP = 504;          // staged edges per warp (48 KB of shared memory per CTA)
+constexpr int TILE_WARPS = 8;
+
+template <int T>
+__global__ void __launch_bounds__(TILE_WARPS * 32, 4) k_sweep_tile(SweepArgs a, int64_t nv) {
+    static_assert(32 * T <= TILE_CAP + 8, "the per-lane fallback layout must fit the buffer");
+    __shared__ int32_t st_all[TILE_WARPS][TILE_CAP + 8];
+    __shared__ double sw_all[TILE_WARPS][TILE_CAP + 8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t *st = st_all[warp];
+    double *sw = sw_all[warp];
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t tile = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile * 32 < nv;
+         tile += nwarps) {
+        const int64_t v64 = tile * 32 + lane;
+        const bool valid = v64 < nv;
+        const int32_t v = (int32_t)v64;
+        int64_t e0 = 0, e1 = 0;
+        if (valid) {
+            e0 = a.rowptr[v];
+            e1 = a.rowptr[v + 1];
+        }
+        const int d = (int)(e1 - e0);
+        const unsigned vm = __ballot_sync(0xffffffffu, valid);
+        const int last = 31 - __clz(vm);
+        const int64_t E0 = __shfl_sync(0xffffffffu, e0, 0);
+        const int64_t E1 = __shfl_sync(0xffffffffu, e1, last);
+        const int64_t A0 = E0 & ~3LL, B0 = E0 & ~1LL;
+        int off_t, off_w; // where this lane's row starts in st / sw
+        if (E1 - A0 <= TILE_CAP) {
+            // coalesced: int4 for tails, double2 for weights (16-byte aligned starts)
+            const int64_t nt = (E1 - A0 + 3) >> 2, nw2 = (E1 - B0 + 1) >> 1;
+            for (int64_t k = lane; k < nt; k += 32) {
+                const int64_t i = A0 + 4 * k;
+                if (i + 4 <= a.ne) {
+                    const int4 x = __ldcs(reinterpret_cast<const int4 *>(a.tail + i));
+                    st[4 * k] = x.x;
+                    st[4 * k + 1] = x.y;
+                    st[4 * k + 2] = x.z;
+                    st[4 * k + 3] = x.w;
+                } else {
+                    for (int q = 0; q < 4 && i + q < a.ne; q++) st[4 * k + q] = __ldcs(a.tail + i + q);
+                }
+            }
+            for (int64_t k = lane; k < nw2; k += 32) {
+                const int64_t i = B0 + 2 * k;
+                if (i + 2 <= a.ne) {
+                    const double2 x = __ldcs(reinterpret_cast<const double2 *>(a.weight + i));
+                    sw[2 * k] = x.x;
+                    sw[2 * k + 1] = x.y;
+                } else if (i < a.ne) {
+                    sw[2 * k] = __ldcs(a.weight + i);
+                }
+            }
+            off_t = (int)(e0 - A0);
+            off_w = (int)(e0 - B0);
+        } else {
+            // long range (hub rows inside the tile): each lane copies its own short row
+            if (valid && d <= T) {
+                for (int j = 0; j < d; j++) {
+                    st[lane * T + j] = __ldcs(a.tail + e0 + j);
+                    sw[lane * T + j] = __ldcs(a.weight + e0 + j);
+                }
+            }
+            off_t = lane * T;
+            off_w = lane * T;
+        }
+        __syncwarp();
+        if (valid && d <= T) {
+            if (a.active && !a.active[v]) {
+                a.cw[v] = a.frozen[v];
+            } else {
+                const int32_t *ts = st + off_t;
+                double *ws = sw + off_w;
+                const int32_t cc = __ldg(a.curr + v);
+                const double vd = a.vdeg[v];
+                const double ccDeg = __ldg(a.cdeg + cc);
+                int32_t c[T];
+                double selfLoop = 0.0;
+#pragma unroll
+                for (int j = 0; j < T; j++) {
+                    c[j] = -1;
+                    if (j < d) c[j] = __ldg(a.curr + ts[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < T; j++)
+                    if (j < d && ts[j] == v) selfLoop = __dadd_rn(selfLoop, ws[j]);
+                uint32_t first = 0;
+#pragma unroll
+                for (int j = 0; j < T; j++) {
+                    if (j < d) {
+                        int fj = j;
+#pragma unroll
+                        for (int k = j - 1; k >= 0; k--)
+                            if (c[k] == c[j]) fj = k;
+                        if (fj == j) first |= 1u << j;
+                        else ws[fj] = __dadd_rn(ws[fj], ws[j]);
+                    }
+                }
+                double counter0 = 0.0;
+#pragma unroll
+                for (int j = 0; j < T; j++)
+                    if (((first >> j) & 1u) && c[j] == cc) counter0 = ws[j];
+                const double eix = __dsub_rn(counter0, selfLoop);
+                const double ax = __dsub_rn(ccDeg, vd);
+                double bg = 0.0;
+                int32_t bc = INT_MAX;
+                bool ok = false;
+#pragma unroll
+                for (int b = 0; b < T; b += 8) {
+                    double ay[8];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        const int j = b + q;
+                        ay[q] = 0.0;
+                        if (((first >> j) & 1u) && c[j] != cc) ay[q] = __ldg(a.cdeg + c[j]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        const int j = b + q;
+                        if (((first >> j) & 1u) && c[j] != cc) {
+                            const double g = gain_of(ws[j], eix, vd, ay[q], ax, a.constant);
+                            if (g > 0.0 && better(true, g, c[j], ok, bg, bc, a.ref)) {
+                                bg = g;
+                                bc = c[j];
+                                ok = true;
+                            }
+                        }
+                    }
+                }
+                int32_t ccSize = 0, bs = 0;
+                if (ok && vg_rid(a.ref, bc) > vg_rid(a.ref, cc)) {
+                    ccSize = __ldg(a.csize + cc);
+                    bs = __ldg(a.csize + bc);
+                }
+                commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, bc, bs);
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -868,7 +1019,8 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
         if (cls == 0 && natural) {
             if (nv == 0) continue;
             LaunchTimer lt(ctx);
-            k_sweep_thread<false, TMAX, TB><<<vg_grid(ctx, nv, TB, 8), TB, 0, ctx->stream>>>(a, nullptr, nv);
+            k_sweep_tile<TMAX><<<vg_grid(ctx, nv, TILE_WARPS * 32, 8), TILE_WARPS * 32, 0,
+                                 ctx->stream>>>(a, nv);
             VG_CHECK_LAUNCH();
             continue;
         }
@@ -999,6 +1151,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         a.frozen = frozen.p;
         a.active = use_et ? active.p : nullptr;
         a.ref = g->ref;
+        a.ne = g->ne;
         a.constant = constant;
         if (timing) VG_CUDA(cudaEventRecord(ev0, ctx->stream));
         for (int64_t ci = 0; ci < numColor; ci++) {

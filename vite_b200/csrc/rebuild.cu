@@ -114,42 +114,14 @@ __global__ void k_new_ids(const int32_t *__restrict__ comm, int64_t nv,
     }
 }
 
-// degree of each vertex in reference order
-__global__ void k_deg_by_ref(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ pos,
-                             int64_t nv, int64_t *__restrict__ deg) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nv;
-         r += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t p = pos[r];
-        deg[r] = rowptr[p + 1] - rowptr[p];
-    }
-}
-
-// triples in reference vertex order, CSR order inside a row
-__global__ void k_triples_ref(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
-                              const double *__restrict__ w, int64_t nv,
-                              const int32_t *__restrict__ pos, const int64_t *__restrict__ off,
-                              const int32_t *__restrict__ new_pos, const int32_t *__restrict__ new_ref,
-                              int32_t *__restrict__ src, int32_t *__restrict__ dst,
-                              double *__restrict__ wo) {
-    const int lane = threadIdx.x & 31;
-    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r = wg; r < nv; r += nw) {
-        const int32_t p = pos[r];
-        const int32_t s = new_pos[p];
-        const int64_t e0 = rowptr[p], len = rowptr[p + 1] - e0, o = off[r];
-        for (int64_t j = lane; j < len; j += 32) {
-            src[o + j] = s;
-            dst[o + j] = new_ref[tail[e0 + j]];
-            wo[o + j] = w[e0 + j];
-        }
-    }
-}
-
 } // namespace
 
+vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
+                            const int32_t *new_row, const int32_t *new_key, int64_t nc,
+                            const int32_t *key_to_pos);
+
 vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm) {
-    const int64_t nv = g->nv, ne = g->ne;
+    const int64_t nv = g->nv;
     const int grid = vg_grid(ctx, nv, 256);
     if (!g->ref) {
         // reference layout: first appearance by position is first appearance by id
@@ -170,16 +142,7 @@ vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm) {
         first.release();
         flag.release();
         rank.release();
-        DevBuf<int32_t> src(ctx, ne), dst(ctx, ne);
-        DevBuf<double> w(ctx, ne);
-        if (ne) {
-            LaunchTimer lt(ctx);
-            k_triples<<<vg_grid(ctx, nv * 32, 256), 256, 0, ctx->stream>>>(
-                g->rowptr, g->tail, g->weight, nv, newof.p, src.p, dst.p, w.p);
-        }
-        VG_CHECK_LAUNCH();
-        newof.release();
-        return vg_csr_from_triples(ctx, nc, src, dst, w, ne, true);
+        return vg_aggregate_rows(ctx, g, nullptr, newof.p, newof.p, nc, nullptr);
     }
     DevBuf<int32_t> first_ref(ctx, nv), first_pos(ctx, nv), flag_ref(ctx, nv), flag_pos(ctx, nv);
     DevBuf<int64_t> rank_ref(ctx, nv), rank_pos(ctx, nv);
@@ -212,26 +175,7 @@ vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm) {
     rank_pos.release();
     first_ref.release();
     first_pos.release();
-    DevBuf<int64_t> off(ctx, nv + 1);
-    VG_CUDA(cudaMemsetAsync(off.p + nv, 0, sizeof(int64_t), ctx->stream));
-    if (nv) {
-        LaunchTimer lt(ctx);
-        k_deg_by_ref<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->pos, nv, off.p);
-    }
-    VG_CHECK_LAUNCH();
-    vg_exclusive_scan_i64(ctx, off.p, nv + 1);
-    DevBuf<int32_t> src(ctx, ne), dst(ctx, ne);
-    DevBuf<double> w(ctx, ne);
-    if (ne) {
-        LaunchTimer lt(ctx);
-        k_triples_ref<<<vg_grid(ctx, nv * 32, 256), 256, 0, ctx->stream>>>(
-            g->rowptr, g->tail, g->weight, nv, g->pos, off.p, new_pos.p, new_ref.p, src.p, dst.p, w.p);
-    }
-    VG_CHECK_LAUNCH();
-    off.release();
-    new_ref.release();
-    new_pos.release();
-    vg_graph *h = vg_csr_from_triples(ctx, nc, src, dst, w, ne, true, next_pos.p);
+    vg_graph *h = vg_aggregate_rows(ctx, g, g->pos, new_pos.p, new_ref.p, nc, next_pos.p);
     // the arrays were sized nv; the next level keeps its first nc entries
     DevBuf<int32_t> r2(ctx, nc), p2(ctx, nc);
     if (nc) {
