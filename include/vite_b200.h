@@ -132,6 +132,25 @@ vg_status vg_graph_reorder(vg_ctx *ctx, vg_graph *g, int32_t mode);
  * weighted degree of every vertex (optional copy out) and 1/(2m). */
 vg_status vg_vertex_degree(vg_ctx *ctx, vg_graph *g, double *vdeg_out, double *constant_out);
 
+/* Allocation-free variant of vg_vertex_degree (no counterpart in the reference,
+ * which allocates with std::vector). For callers that cannot allocate device memory
+ * while they run -- a server that reserved its whole memory budget at start-up, a
+ * framework whose allocator owns the device memory, code that must not stall or fail
+ * on an allocation mid-run. The caller passes device pointers: rowptr int64[nv+1]
+ * and weights f64[ne] of a CSR, and vdeg_out f64[nv] for the degrees; 1/(2m) is
+ * written to *constant_out (host). Runs on `stream` (a cudaStream_t, NULL = default
+ * stream) of the current device and returns after the stream has finished. The
+ * scratch of the reduction is a file-scope device array of 512 KiB held by every GPU
+ * that loads the library: at most VG_NOALLOC_MAX_VERTICES vertices, larger graphs
+ * are rejected with VG_ERR_ARG. All calls share that array, so calls that overlap on
+ * the GPU race. The first call on a device looks the array's address up with that
+ * device current; make it before any stream capture. errbuf (may be NULL) receives a
+ * message on failure. Allocates nothing: no cudaMalloc, no cudaFree. */
+#define VG_NOALLOC_MAX_VERTICES (2048LL * 65536LL)
+vg_status vg_vertex_degree_noalloc(int64_t nv, const int64_t *d_rowptr, const double *d_weight,
+                                   double *d_vdeg_out, double *constant_out, void *stream,
+                                   char *errbuf, size_t errlen);
+
 /* --- the Louvain path ----------------------------------------------------------- */
 
 /* One Louvain phase: distLouvainMethod / ...WithColoring / ...VertexOrder

@@ -34,7 +34,7 @@ EXPORTED_SYMBOLS = [
     "vg_graph_upload", "vg_graph_info", "vg_graph_download", "vg_graph_free", "vg_vertex_degree",
     "vg_louvain_phase", "vg_color", "vg_set_colors", "vg_rebuild", "vg_louvain_run",
     "vg_generate_rgg", "vg_generate_ba", "vg_generate_er", "vg_graph_reweight",
-    "vg_graph_reorder",
+    "vg_graph_reorder", "vg_vertex_degree_noalloc",
 ]
 
 
@@ -112,6 +112,8 @@ def lib() -> C.CDLL:
         L.vg_generate_er.argtypes = [vp, C.c_int64, C.c_double, C.c_uint64, C.POINTER(vp)]
         L.vg_graph_reweight.argtypes = [vp, vp, C.c_int32, C.c_uint64]
         L.vg_graph_reorder.argtypes = [vp, vp, C.c_int32]
+        L.vg_vertex_degree_noalloc.argtypes = [C.c_int64, vp, vp, vp, _f64p, vp, C.c_char_p,
+                                               C.c_size_t]
         for name in EXPORTED_SYMBOLS:
             if name not in ("vg_last_error", "vg_ctx_bytes_in_use"):
                 getattr(L, name).restype = C.c_int
@@ -121,6 +123,23 @@ def lib() -> C.CDLL:
 
 def _ptr(a: np.ndarray | None, ty=_i64p):
     return None if a is None else a.ctypes.data_as(ty)
+
+
+NOALLOC_MAX_VERTICES = 2048 * 65536
+
+
+def vertex_degree_noalloc(nv: int, d_rowptr: int, d_weight: int, d_vdeg_out: int,
+                          stream: int = 0) -> float:
+    """vg_vertex_degree_noalloc: degrees into the caller's device buffer d_vdeg_out
+    (device pointers as integers, e.g. torch tensor .data_ptr()); returns 1/(2m).
+    Allocates no device memory; see include/vite_b200.h for the limits."""
+    err = C.create_string_buffer(512)
+    c = C.c_double()
+    st = lib().vg_vertex_degree_noalloc(nv, d_rowptr, d_weight, d_vdeg_out, C.byref(c),
+                                        stream or None, err, len(err))
+    if st != VG_OK:
+        raise VgError(st, err.value.decode())
+    return c.value
 
 
 @dataclass
