@@ -186,6 +186,47 @@ vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g, const vg_run_params *p,
                          vg_level_stat *levels, int32_t max_levels, int32_t *nlevels_out,
                          int64_t *comm_out);
 
+/* --- batched and served runs ---------------------------------------------------
+ * No counterpart in the reference, which runs one graph per job: many
+ * independent graphs run as one packed graph, each with the level loop of
+ * vg_louvain_run (plain phase, threshold, one_phase, layout) and the same
+ * results as a run of its own. One step = one round: admit queued graphs while
+ * their estimated footprint fits the budget, run one phase for every graph in
+ * the batch, retire the graphs whose level loop ended, rebuild the rest. */
+typedef struct vg_batch vg_batch;
+
+/* the batch frees the submitted graph once it has been packed */
+#define VG_BATCH_TAKE 1
+/* keep the composed community of every vertex (vg_batch_result comm_out) */
+#define VG_BATCH_COMM 2
+
+typedef struct vg_batch_stats {
+    int64_t submitted, admitted, completed, rounds;
+    int64_t running, queued;
+    size_t running_bytes;          /* estimated footprint of the running graphs */
+    double seconds_phase, seconds_rebuild;
+} vg_batch_stats;
+
+/* budget_bytes = 0: admit every queued graph at the next step */
+vg_status vg_batch_create(vg_ctx *ctx, size_t budget_bytes, vg_batch **out);
+vg_status vg_batch_destroy(vg_batch *b);
+/* Queue a graph; it must stay valid until packed (the next step), or be handed
+ * over with VG_BATCH_TAKE. Rejected when p asks for coloring, vertex ordering,
+ * early termination or threshold cycling, or when the graph alone exceeds the
+ * budget. */
+vg_status vg_batch_submit(vg_batch *b, vg_graph *g, const vg_run_params *p, int32_t flags,
+                          int64_t *job_out);
+vg_status vg_batch_step(vg_batch *b, int32_t *running_out, int32_t *queued_out);
+/* ids of the graphs finished since the last poll */
+vg_status vg_batch_poll(vg_batch *b, int64_t *ids, int32_t max_ids, int32_t *n_out);
+/* per-level statistics (the phase and rebuild times are the shared round's)
+ * and, with VG_BATCH_COMM, the communities as vg_louvain_run's comm_out */
+vg_status vg_batch_result(vg_batch *b, int64_t job, vg_level_stat *levels, int32_t max_levels,
+                          int32_t *nlevels_out, int64_t *comm_out);
+/* drop a finished graph's results */
+vg_status vg_batch_forget(vg_batch *b, int64_t job);
+vg_status vg_batch_get_stats(vg_batch *b, vg_batch_stats *out);
+
 /* --- generators --------------------------------------------------------------- */
 
 /* generateInMemGraph for one rank (distgraph.cpp:391-407, 412-983): n points

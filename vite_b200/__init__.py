@@ -35,7 +35,12 @@ EXPORTED_SYMBOLS = [
     "vg_louvain_phase", "vg_color", "vg_set_colors", "vg_rebuild", "vg_louvain_run",
     "vg_generate_rgg", "vg_generate_ba", "vg_generate_er", "vg_graph_reweight",
     "vg_graph_reorder", "vg_vertex_degree_noalloc",
+    "vg_batch_create", "vg_batch_destroy", "vg_batch_submit", "vg_batch_step", "vg_batch_poll",
+    "vg_batch_result", "vg_batch_forget", "vg_batch_get_stats",
 ]
+
+VG_BATCH_TAKE = 1
+VG_BATCH_COMM = 2
 
 
 class VgError(RuntimeError):
@@ -63,6 +68,16 @@ class LevelStat(C.Structure):
                 ("seconds_color", C.c_double), ("seconds_phase", C.c_double),
                 ("seconds_sweep", C.c_double), ("seconds_rebuild", C.c_double),
                 ("edges_swept", C.c_int64), ("seconds_layout", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
+                ("rounds", C.c_int64), ("running", C.c_int64), ("queued", C.c_int64),
+                ("running_bytes", C.c_size_t), ("seconds_phase", C.c_double),
+                ("seconds_rebuild", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -114,6 +129,15 @@ def lib() -> C.CDLL:
         L.vg_graph_reorder.argtypes = [vp, vp, C.c_int32]
         L.vg_vertex_degree_noalloc.argtypes = [C.c_int64, vp, vp, vp, _f64p, vp, C.c_char_p,
                                                C.c_size_t]
+        L.vg_batch_create.argtypes = [vp, C.c_size_t, C.POINTER(vp)]
+        L.vg_batch_destroy.argtypes = [vp]
+        L.vg_batch_submit.argtypes = [vp, vp, C.POINTER(RunParams), C.c_int32, _i64p]
+        L.vg_batch_step.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.vg_batch_poll.argtypes = [vp, _i64p, C.c_int32, C.POINTER(C.c_int32)]
+        L.vg_batch_result.argtypes = [vp, C.c_int64, C.POINTER(LevelStat), C.c_int32,
+                                      C.POINTER(C.c_int32), _i64p]
+        L.vg_batch_forget.argtypes = [vp, C.c_int64]
+        L.vg_batch_get_stats.argtypes = [vp, C.POINTER(BatchStats)]
         for name in EXPORTED_SYMBOLS:
             if name not in ("vg_last_error", "vg_ctx_bytes_in_use"):
                 getattr(L, name).restype = C.c_int
@@ -332,6 +356,113 @@ class Context:
         self._check(lib().vg_louvain_run(self.handle, g.handle, C.byref(p), stats, max_levels,
                                          C.byref(n), _ptr(comm)))
         return Levels([stats[i].as_dict() for i in range(min(n.value, max_levels))], comm)
+
+    def batch(self, budget: int = 0) -> "Batch":
+        return Batch(self, budget)
+
+    def run_batch(self, graphs: list, threshold: float = 1e-6, want_comm: bool = False,
+                  one_phase: bool = False, layout: int = 2) -> list:
+        """Run every graph to completion as one batch; one Levels per graph, in order."""
+        with Batch(self) as b:
+            ids = [b.submit(g, threshold=threshold, one_phase=one_phase, want_comm=want_comm,
+                            layout=layout) for g in graphs]
+            b.run_all()
+            return [b.result(j, want_comm=want_comm) for j in ids]
+
+
+class Batch:
+    """vg_batch: many graphs run together (batched and served Louvain).
+
+    ``submit`` queues a graph with its run parameters; every ``step`` is one round
+    (admit what fits the budget, one phase for every graph in the batch, retire
+    the graphs whose level loop ended, rebuild the rest); ``poll`` lists the
+    graphs finished since the last poll and ``result`` returns what ``Context.run``
+    would have returned for the graph alone.
+    """
+
+    def __init__(self, ctx: "Context", budget: int = 0):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx._check(lib().vg_batch_create(ctx.handle, budget, C.byref(h)))
+        self.handle = h
+        self._nv: dict[int, int] = {}
+        self._held: dict[int, Graph] = {}
+
+    def submit(self, g: Graph, threshold: float = 1e-6, one_phase: bool = False,
+               want_comm: bool = False, take: bool = False, layout: int = 2) -> int:
+        """Queue g. With take=True the batch frees g once packed (g is emptied);
+        otherwise g must stay alive until it is packed (the batch keeps a
+        reference until the graph's job is polled as finished)."""
+        p = RunParams(threshold, 0, 0, 8, 0, 0, 1.0, 0, int(one_phase), layout)
+        flags = (VG_BATCH_TAKE if take else 0) | (VG_BATCH_COMM if want_comm else 0)
+        jid = C.c_int64()
+        nv = g.nv
+        self.ctx._check(lib().vg_batch_submit(self.handle, g.handle, C.byref(p), flags,
+                                              C.byref(jid)))
+        if take:
+            g.handle = None
+        else:
+            self._held[jid.value] = g
+        self._nv[jid.value] = nv
+        return jid.value
+
+    def step(self) -> tuple[int, int]:
+        r, q = C.c_int32(), C.c_int32()
+        self.ctx._check(lib().vg_batch_step(self.handle, C.byref(r), C.byref(q)))
+        return r.value, q.value
+
+    def poll(self, max_ids: int = 65536) -> list[int]:
+        ids = np.empty(max_ids, np.int64)
+        n = C.c_int32()
+        self.ctx._check(lib().vg_batch_poll(self.handle, _ptr(ids), max_ids, C.byref(n)))
+        done = [int(x) for x in ids[:n.value]]
+        for j in done:  # packed long ago: the caller's graph may go
+            self._held.pop(j, None)
+        return done
+
+    def result(self, jid: int, want_comm: bool = False, max_levels: int = 256) -> Levels:
+        stats = (LevelStat * max_levels)()
+        n = C.c_int32()
+        comm = np.empty(self._nv[jid], np.int64) if want_comm else None
+        self.ctx._check(lib().vg_batch_result(self.handle, jid, stats, max_levels, C.byref(n),
+                                              _ptr(comm)))
+        return Levels([stats[i].as_dict() for i in range(min(n.value, max_levels))], comm)
+
+    def forget(self, jid: int) -> None:
+        self.ctx._check(lib().vg_batch_forget(self.handle, jid))
+        self._nv.pop(jid, None)
+
+    def stats(self) -> dict:
+        s = BatchStats()
+        self.ctx._check(lib().vg_batch_get_stats(self.handle, C.byref(s)))
+        return s.as_dict()
+
+    def run_all(self) -> None:
+        """Step until nothing is queued or running."""
+        while True:
+            r, q = self.step()
+            if r == 0 and q == 0:
+                break
+
+    def close(self) -> None:
+        if self.handle:
+            self.ctx._check(lib().vg_batch_destroy(self.handle))
+            self.handle = None
+        self._held = {}
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            if self.handle:
+                lib().vg_batch_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
 
 
 @dataclass

@@ -66,7 +66,22 @@ struct SweepArgs {
     const int32_t *__restrict__ ref;     // reference id of each position (null: identity)
     int64_t ne;                          // CSR entries (bounds of the vector loads)
     double constant;
+    // batched graphs (null for one graph): the graph of each vertex, each graph's
+    // 1/(2m), and the graphs whose phase has ended (their vertices are skipped)
+    const int32_t *__restrict__ vjob = nullptr;
+    const double *__restrict__ jconst = nullptr;
+    const uint8_t *__restrict__ jdone = nullptr;
 };
+
+// the constant of v's graph; false when v belongs to a graph whose phase has ended
+__device__ __forceinline__ bool vertex_live(const SweepArgs &a, int32_t v, double &cst) {
+    cst = a.constant;
+    if (!a.vjob) return true;
+    const int32_t j = __ldg(a.vjob + v);
+    if (__ldg(a.jdone + j)) return false;
+    cst = __ldg(a.jconst + j);
+    return true;
+}
 
 // gain of moving to a community (louvain.cpp:2263), evaluated in the reference's order
 __device__ __forceinline__ double gain_of(double eiy, double eix, double vd, double ay, double ax,
@@ -132,6 +147,8 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? 3 : 3)) k_sweep_thread(
         const int64_t e0 = a.rowptr[v];
         const int d = (int)(a.rowptr[v + 1] - e0);
         if (!LIST && d > T) continue; // the list kernels take the larger degrees
+        double cst;
+        if (!vertex_live(a, v, cst)) continue;
         if (a.active && !a.active[v]) {
             a.cw[v] = a.frozen[v];
             continue;
@@ -193,7 +210,7 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? 3 : 3)) k_sweep_thread(
             for (int q = 0; q < 8; q++) {
                 const int j = b + q;
                 if (((first >> j) & 1u) && c[j] != cc) {
-                    const double g = gain_of(ssum[j][tid], eix, vd, ay[q], ax, a.constant);
+                    const double g = gain_of(ssum[j][tid], eix, vd, ay[q], ax, cst);
                     if (g > 0.0 && better(true, g, c[j], ok, bg, bc, a.ref)) {
                         bg = g;
                         bc = c[j];
@@ -236,8 +253,11 @@ __global__ void __launch_bounds__(TILE_WARPS * 32, 4) k_sweep_tile(SweepArgs a, 
     for (int64_t tile = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile * 32 < nv;
          tile += nwarps) {
         const int64_t v64 = tile * 32 + lane;
-        const bool valid = v64 < nv;
         const int32_t v = (int32_t)v64;
+        const bool valid = v64 < nv;
+        double cst = a.constant;
+        const bool live = valid && vertex_live(a, v, cst);
+        if (!__any_sync(0xffffffffu, live)) continue;
         int64_t e0 = 0, e1 = 0;
         if (valid) {
             e0 = a.rowptr[v];
@@ -279,7 +299,7 @@ __global__ void __launch_bounds__(TILE_WARPS * 32, 4) k_sweep_tile(SweepArgs a, 
             off_w = (int)(e0 - B0);
         } else {
             // long range (hub rows inside the tile): each lane copies its own short row
-            if (valid && d <= T) {
+            if (live && d <= T) {
                 for (int j = 0; j < d; j++) {
                     st[lane * T + j] = __ldcs(a.tail + e0 + j);
                     sw[lane * T + j] = __ldcs(a.weight + e0 + j);
@@ -289,7 +309,7 @@ __global__ void __launch_bounds__(TILE_WARPS * 32, 4) k_sweep_tile(SweepArgs a, 
             off_w = lane * T;
         }
         __syncwarp();
-        if (valid && d <= T) {
+        if (live && d <= T) {
             if (a.active && !a.active[v]) {
                 a.cw[v] = a.frozen[v];
             } else {
@@ -342,7 +362,7 @@ __global__ void __launch_bounds__(TILE_WARPS * 32, 4) k_sweep_tile(SweepArgs a, 
                     for (int q = 0; q < 8; q++) {
                         const int j = b + q;
                         if (((first >> j) & 1u) && c[j] != cc) {
-                            const double g = gain_of(ws[j], eix, vd, ay[q], ax, a.constant);
+                            const double g = gain_of(ws[j], eix, vd, ay[q], ax, cst);
                             if (g > 0.0 && better(true, g, c[j], ok, bg, bc, a.ref)) {
                                 bg = g;
                                 bc = c[j];
@@ -392,6 +412,8 @@ __global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t idx = wg; idx < count; idx += nw) {
         const int32_t v = list[idx];
+        double cst;
+        if (!vertex_live(a, v, cst)) continue;
         const int32_t cc = a.curr[v];
         if (a.active && !a.active[v]) {
             if (lane == 0) a.cw[v] = a.frozen[v];
@@ -483,7 +505,7 @@ __global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
             double ay;
             int32_t sz;
             load_comm(a, kk, ay, sz);
-            const double g = gain_of(vals[s], eix, vd, ay, ax, a.constant);
+            const double g = gain_of(vals[s], eix, vd, ay, ax, cst);
             if (g > 0.0 && better(true, g, kk, ok, gain, cand, a.ref)) {
                 gain = g;
                 cand = kk;
@@ -544,6 +566,8 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
     }
     for (int64_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
         const int32_t v = list[idx];
+        double cst;
+        if (!vertex_live(a, v, cst)) continue;
         const int32_t cc = a.curr[v];
         if (a.active && !a.active[v]) {
             if (threadIdx.x == 0) a.cw[v] = a.frozen[v];
@@ -641,7 +665,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
             double ay;
             int32_t sz;
             load_comm(a, kk, ay, sz);
-            const double g = gain_of(vals[s], eix, vd, ay, ax, a.constant);
+            const double g = gain_of(vals[s], eix, vd, ay, ax, cst);
             if (g > 0.0 && better(true, g, kk, ok, gain, cand, a.ref)) {
                 gain = g;
                 cand = kk;
@@ -740,71 +764,213 @@ __device__ double block_sum(double v, double *ws) {
     return s;
 }
 
-constexpr int APPLY_BLOCKS = 592; // 4 per SM on a 148-SM part; fixed so sums are reproducible
-constexpr int APPLY_THREADS = 512;
+// ---------------------------------------------------------------------------------
+// Fixed-order segmented sums. A segment (the vertex range of one graph) is cut
+// into chunks of SEG_CHUNK entries counted from the segment's start; thread t of
+// a chunk's block adds entries t, t + SEG_THREADS, ... in order and the warps
+// combine through a fixed shuffle tree; a segment's chunk partials are then
+// combined the same way by one block of SEG_FINAL threads. The order depends only
+// on the segment's own length, so a graph's 2m and modularity sums are the same
+// bits whether it runs alone or packed with other graphs.
 
-// distUpdateLocalCinfo (louvain.cpp:2534-2547) fused with the two sums of
-// distComputeModularity (louvain.cpp:2496-2504) and the frozen-vertex count
-__global__ void __launch_bounds__(APPLY_THREADS) k_apply_mod(
-    int64_t nv, double *__restrict__ cdeg, int32_t *__restrict__ csize, CommInfo *__restrict__ cupd,
-    const double *__restrict__ cw, const uint8_t *__restrict__ active, int do_sums,
-    double *__restrict__ part) {
-    __shared__ double ws[32];
-    double le = 0.0, la2 = 0.0, frozen = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const CommInfo u = cupd[i];
-        double cd;
-        if (u.size != 0 || u.deg != 0.0) {
-            cd = __dadd_rn(cdeg[i], u.deg);
-            cdeg[i] = cd;
-            csize[i] += u.size;
-            CommInfo z;
-            z.deg = 0.0;
-            z.size = 0;
-            z.pad = 0;
-            cupd[i] = z;
-        } else {
-            cd = do_sums ? cdeg[i] : 0.0;
-        }
-        if (do_sums) {
-            le = __dadd_rn(le, cw[i]);
-            la2 = __dadd_rn(la2, __dmul_rn(cd, cd));
-            if (active && !active[i]) frozen += 1.0;
-        }
+constexpr int SEG_CHUNK = 2048;
+constexpr int SEG_THREADS = 256;
+constexpr int SEG_FINAL = 1024;
+
+// largest j with cb[j] <= q (cb[0] = 0 <= q < cb[J])
+__device__ __forceinline__ int64_t seg_of_chunk(const int64_t *__restrict__ cb, int64_t J, int64_t q) {
+    int64_t lo = 0, hi = J;
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (cb[mid] <= q) lo = mid;
+        else hi = mid;
     }
-    if (!do_sums) return;
-    le = block_sum(le, ws);
-    la2 = block_sum(la2, ws);
-    frozen = block_sum(frozen, ws);
-    if (threadIdx.x == 0) {
-        part[3 * blockIdx.x + 0] = le;
-        part[3 * blockIdx.x + 1] = la2;
-        part[3 * blockIdx.x + 2] = frozen;
+    return lo;
+}
+
+__global__ void __launch_bounds__(SEG_THREADS) k_seg_sum_chunks(
+    const double *__restrict__ x, const int64_t *__restrict__ voff, const int64_t *__restrict__ cb,
+    int64_t J, int64_t C, double *__restrict__ part) {
+    __shared__ double ws[32];
+    for (int64_t q = blockIdx.x; q < C; q += gridDim.x) {
+        const int64_t j = seg_of_chunk(cb, J, q);
+        const int64_t lo = voff[j] + (q - cb[j]) * SEG_CHUNK;
+        const int64_t hi = min(lo + SEG_CHUNK, voff[j + 1]);
+        double s = 0.0;
+        for (int64_t i = lo + threadIdx.x; i < hi; i += SEG_THREADS) s = __dadd_rn(s, x[i]);
+        s = block_sum(s, ws);
+        if (threadIdx.x == 0) part[q] = s;
     }
 }
 
-// final reduction and the ABS_MOD_PER_ITER modularity (louvain.cpp:2518-2524)
-__global__ void k_mod_final(const double *__restrict__ part, int nblk, double constant,
-                            double *__restrict__ out) {
+__global__ void __launch_bounds__(SEG_FINAL) k_seg_sum_final(const double *__restrict__ part,
+                                                             const int64_t *__restrict__ cb,
+                                                             int64_t J, double *__restrict__ out) {
     __shared__ double ws[32];
-    double le = 0.0, la2 = 0.0, fr = 0.0;
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-        le = __dadd_rn(le, part[3 * b]);
-        la2 = __dadd_rn(la2, part[3 * b + 1]);
-        fr += part[3 * b + 2];
+    for (int64_t j = blockIdx.x; j < J; j += gridDim.x) {
+        double s = 0.0;
+        for (int64_t q = cb[j] + threadIdx.x; q < cb[j + 1]; q += SEG_FINAL) s = __dadd_rn(s, part[q]);
+        s = block_sum(s, ws);
+        if (threadIdx.x == 0) out[j] = s;
     }
-    le = block_sum(le, ws);
-    la2 = block_sum(la2, ws);
-    fr = block_sum(fr, ws);
-    if (threadIdx.x == 0) {
-        const double m = __dsub_rn(__dmul_rn(le, constant),
-                                   __dmul_rn(__dmul_rn(la2, constant), constant));
-        out[0] = fabs(m);
-        out[1] = fr;
-        out[2] = le;
-        out[3] = la2;
+}
+
+// distUpdateLocalCinfo (louvain.cpp:2534-2547) fused with the two sums of
+// distComputeModularity (louvain.cpp:2496-2504) and the frozen-vertex count,
+// per chunk of each segment; segments whose phase has ended are skipped
+__global__ void __launch_bounds__(SEG_THREADS) k_apply_seg(
+    const int64_t *__restrict__ voff, const int64_t *__restrict__ cb, int64_t J, int64_t C,
+    double *__restrict__ cdeg, int32_t *__restrict__ csize, CommInfo *__restrict__ cupd,
+    const double *__restrict__ cw, const uint8_t *__restrict__ active,
+    const uint8_t *__restrict__ jdone, int do_sums, double *__restrict__ part) {
+    __shared__ double ws[32];
+    for (int64_t q = blockIdx.x; q < C; q += gridDim.x) {
+        const int64_t j = seg_of_chunk(cb, J, q);
+        if (jdone && jdone[j]) continue;
+        const int64_t lo = voff[j] + (q - cb[j]) * SEG_CHUNK;
+        const int64_t hi = min(lo + SEG_CHUNK, voff[j + 1]);
+        double le = 0.0, la2 = 0.0, frozen = 0.0;
+        for (int64_t i = lo + threadIdx.x; i < hi; i += SEG_THREADS) {
+            const CommInfo u = cupd[i];
+            double cd;
+            if (u.size != 0 || u.deg != 0.0) {
+                cd = __dadd_rn(cdeg[i], u.deg);
+                cdeg[i] = cd;
+                csize[i] += u.size;
+                CommInfo z;
+                z.deg = 0.0;
+                z.size = 0;
+                z.pad = 0;
+                cupd[i] = z;
+            } else {
+                cd = do_sums ? cdeg[i] : 0.0;
+            }
+            if (do_sums) {
+                le = __dadd_rn(le, cw[i]);
+                la2 = __dadd_rn(la2, __dmul_rn(cd, cd));
+                if (active && !active[i]) frozen += 1.0;
+            }
+        }
+        if (!do_sums) continue;
+        le = block_sum(le, ws);
+        la2 = block_sum(la2, ws);
+        frozen = block_sum(frozen, ws);
+        if (threadIdx.x == 0) {
+            part[3 * q + 0] = le;
+            part[3 * q + 1] = la2;
+            part[3 * q + 2] = frozen;
+        }
     }
+}
+
+// per-graph phase state of a batch: the loop test of distLouvainMethod
+// (louvain.cpp:553-563) evaluated for every graph on the device
+struct BatchDecide {
+    double *prev_mod;      // prevMod, starts at `lower`
+    const double *lower;
+    const double *thresh;
+    int32_t *iters;
+    uint8_t *done;
+    int8_t *resbuf;        // which of the three community buffers held pastComm at the break
+    int32_t *live_count;   // graphs still iterating after this iteration
+    int32_t iter;
+    int32_t past_idx;
+};
+
+// final reduction and the ABS_MOD_PER_ITER modularity (louvain.cpp:2518-2524),
+// one block per segment. One graph: out = {Q, frozen, le, la2}; a batch: the
+// loop test per graph
+__global__ void __launch_bounds__(SEG_FINAL) k_mod_seg(const double *__restrict__ part,
+                                                       const int64_t *__restrict__ cb, int64_t J,
+                                                       double constant,
+                                                       const double *__restrict__ jconst,
+                                                       double *__restrict__ out, BatchDecide bd) {
+    __shared__ double ws[32];
+    for (int64_t j = blockIdx.x; j < J; j += gridDim.x) {
+        if (bd.done && bd.done[j]) continue;
+        double le = 0.0, la2 = 0.0, fr = 0.0;
+        for (int64_t q = cb[j] + threadIdx.x; q < cb[j + 1]; q += SEG_FINAL) {
+            le = __dadd_rn(le, part[3 * q]);
+            la2 = __dadd_rn(la2, part[3 * q + 1]);
+            fr += part[3 * q + 2];
+        }
+        le = block_sum(le, ws);
+        la2 = block_sum(la2, ws);
+        fr = block_sum(fr, ws);
+        if (threadIdx.x == 0) {
+            const double c = jconst ? jconst[j] : constant;
+            const double m = fabs(__dsub_rn(__dmul_rn(le, c), __dmul_rn(__dmul_rn(la2, c), c)));
+            if (!bd.done) {
+                out[0] = m;
+                out[1] = fr;
+                out[2] = le;
+                out[3] = la2;
+            } else {
+                bd.iters[j] = bd.iter;
+                if (__dsub_rn(m, bd.prev_mod[j]) < bd.thresh[j]) {
+                    bd.done[j] = 1;
+                    bd.resbuf[j] = (int8_t)bd.past_idx;
+                } else {
+                    bd.prev_mod[j] = m < bd.lower[j] ? bd.lower[j] : m;
+                    atomicAdd(bd.live_count, 1);
+                }
+            }
+        }
+    }
+}
+
+struct SegTable {
+    DevBuf<int64_t> voff, cb; // J + 1 each
+    int64_t J = 0, C = 0;
+};
+
+void seg_table_build(vg_ctx *ctx, const int64_t *h_voff, int64_t J, SegTable &t) {
+    std::vector<int64_t> cb(J + 1, 0);
+    for (int64_t j = 0; j < J; j++)
+        cb[j + 1] = cb[j] + (h_voff[j + 1] - h_voff[j] + SEG_CHUNK - 1) / SEG_CHUNK;
+    t.J = J;
+    t.C = cb[J];
+    t.voff.alloc(ctx, J + 1);
+    t.cb.alloc(ctx, J + 1);
+    VG_CUDA(cudaMemcpyAsync(t.voff.p, h_voff, sizeof(int64_t) * (J + 1), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    VG_CUDA(cudaMemcpyAsync(t.cb.p, cb.data(), sizeof(int64_t) * (J + 1), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    vg_sync(ctx); // the host vectors go out of scope
+}
+
+int seg_grid(vg_ctx *ctx, int64_t chunks) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 8LL * ctx->sm_count));
+}
+
+// per-segment sums of x into out[J] (device)
+void seg_sums(vg_ctx *ctx, const double *x, const SegTable &t, double *out) {
+    DevBuf<double> part(ctx, std::max<int64_t>(t.C, 1));
+    if (t.C) {
+        LaunchTimer lt(ctx);
+        k_seg_sum_chunks<<<seg_grid(ctx, t.C), SEG_THREADS, 0, ctx->stream>>>(x, t.voff.p, t.cb.p,
+                                                                               t.J, t.C, part.p);
+    }
+    VG_CHECK_LAUNCH();
+    {
+        LaunchTimer lt(ctx);
+        k_seg_sum_final<<<(int)std::min<int64_t>(std::max<int64_t>(t.J, 1), 65535), SEG_FINAL, 0,
+                          ctx->stream>>>(part.p, t.cb.p, t.J, out);
+    }
+    VG_CHECK_LAUNCH();
+}
+
+// 2m of one graph in the segmented order
+double twice_m_one(vg_ctx *ctx, const double *vdeg, int64_t nv) {
+    const int64_t voff[2] = {0, nv};
+    SegTable t;
+    seg_table_build(ctx, voff, 1, t);
+    DevBuf<double> out(ctx, 1);
+    seg_sums(ctx, vdeg, t, out.p);
+    double *h = (double *)vg_pinned(ctx, sizeof(double));
+    VG_CUDA(cudaMemcpyAsync(h, out.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    vg_sync(ctx);
+    return *h;
 }
 
 // early termination -t 1/3 (louvain.cpp:172-184): C++'s chained
@@ -1099,7 +1265,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         }
         VG_CHECK_LAUNCH();
     }
-    const double twice_m = nv ? vg_sum_f64(ctx, vdeg.p, nv) : 0.0;
+    const double twice_m = nv ? twice_m_one(ctx, vdeg.p, nv) : 0.0;
     const double constant = 1.0 / twice_m; // distCalcConstantForSecondTerm (louvain.cpp:2217)
     if (nv) {
         LaunchTimer lt(ctx);
@@ -1121,7 +1287,13 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         gt.keys.alloc(ctx, (size_t)cap * gt.blocks);
         gt.vals.alloc(ctx, (size_t)cap * gt.blocks);
     }
-    DevBuf<double> part(ctx, 3 * APPLY_BLOCKS);
+    SegTable seg;
+    {
+        const int64_t voff[2] = {0, nv};
+        seg_table_build(ctx, voff, 1, seg);
+    }
+    DevBuf<double> part(ctx, 3 * std::max<int64_t>(seg.C, 1));
+    const int agrid = seg_grid(ctx, seg.C);
     DevBuf<double> modv(ctx, 4);
     double *hmod = (double *)vg_pinned(ctx, 4 * sizeof(double));
 
@@ -1137,7 +1309,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
     }
     for (;;) {
         numIters++;
-        SweepArgs a;
+        SweepArgs a{};
         a.rowptr = g->rowptr;
         a.tail = g->tail;
         a.weight = g->weight;
@@ -1158,8 +1330,9 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
             sweep_color(ctx, a, bk, ci, gt, ordering == 0, nv);
             if (ordering == 1 && nv) { // per-color community update (louvain.cpp:724-735)
                 LaunchTimer lt(ctx);
-                k_apply_mod<<<APPLY_BLOCKS, APPLY_THREADS, 0, ctx->stream>>>(
-                    nv, cdeg.p, csize.p, cupd.p, cw.p, a.active, 0, part.p);
+                k_apply_seg<<<agrid, SEG_THREADS, 0, ctx->stream>>>(
+                    seg.voff.p, seg.cb.p, 1, seg.C, cdeg.p, csize.p, cupd.p, cw.p, a.active,
+                    nullptr, 0, part.p);
                 VG_CHECK_LAUNCH();
             }
         }
@@ -1167,13 +1340,15 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         if (nv) {
             {
                 LaunchTimer lt(ctx);
-                k_apply_mod<<<APPLY_BLOCKS, APPLY_THREADS, 0, ctx->stream>>>(
-                    nv, cdeg.p, csize.p, cupd.p, cw.p, a.active, 1, part.p);
+                k_apply_seg<<<agrid, SEG_THREADS, 0, ctx->stream>>>(
+                    seg.voff.p, seg.cb.p, 1, seg.C, cdeg.p, csize.p, cupd.p, cw.p, a.active,
+                    nullptr, 1, part.p);
             }
             VG_CHECK_LAUNCH();
             {
                 LaunchTimer lt(ctx);
-                k_mod_final<<<1, 512, 0, ctx->stream>>>(part.p, APPLY_BLOCKS, constant, modv.p);
+                k_mod_seg<<<1, SEG_FINAL, 0, ctx->stream>>>(part.p, seg.cb.p, 1, constant, nullptr,
+                                                           modv.p, BatchDecide{});
             }
             VG_CHECK_LAUNCH();
             VG_CUDA(cudaMemcpyAsync(hmod, modv.p, 2 * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1230,6 +1405,173 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
     else g->comm = C.detach();
     *mod_out = prevMod;
     *iters_out = numIters;
+}
+
+namespace {
+
+// result of graph j = the buffer that held pastComm when its loop ended
+__global__ void k_gather_result(int64_t nv, const int32_t *__restrict__ vjob,
+                                const int8_t *__restrict__ resbuf, const int32_t *__restrict__ b0,
+                                const int32_t *__restrict__ b1, const int32_t *__restrict__ b2,
+                                int32_t *__restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int r = resbuf[vjob[i]];
+        out[i] = r == 0 ? b0[i] : (r == 1 ? b1[i] : b2[i]);
+    }
+}
+
+} // namespace
+
+// One Louvain phase (plain distLouvainMethod, louvain.cpp:427-591) for each of the
+// J graphs packed in U (graph j owns vertices [voff[j], voff[j+1]) and only
+// references its own vertices). Every graph keeps its own 1/(2m), modularity,
+// loop test and iteration count; a graph whose loop has ended is skipped by all
+// later launches. Results: U->comm (each graph's pastComm at its break),
+// mod_out[j] (prevMod) and iters_out[j].
+void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t *h_voff,
+                             const int32_t *vjob, const double *h_thresh, const double *h_lower,
+                             double *mod_out, int32_t *iters_out, double *sweep_ms) {
+    configure_kernels_once();
+    const int64_t nv = U->nv;
+    VG_REQUIRE(J >= 1 && nv >= J, "a batch needs at least one vertex per graph");
+    SegTable seg;
+    seg_table_build(ctx, h_voff, J, seg);
+    DevBuf<double> vdeg(ctx, nv), cw(ctx, nv), cdeg(ctx, nv);
+    DevBuf<int32_t> csize(ctx, nv);
+    DevBuf<CommInfo> cupd(ctx, nv);
+    DevBuf<int32_t> B0(ctx, nv), B1(ctx, nv), B2(ctx, nv);
+    const int grid = vg_grid(ctx, nv, 256);
+    {
+        LaunchTimer lt(ctx);
+        k_degree<<<grid, 256, 0, ctx->stream>>>(U->rowptr, U->weight, nv, vdeg.p);
+    }
+    VG_CHECK_LAUNCH();
+    // per-graph 2m in each graph's own fixed order, 1/(2m) on the host as in the plain path
+    DevBuf<double> jconst(ctx, J);
+    {
+        DevBuf<double> tm(ctx, J);
+        seg_sums(ctx, vdeg.p, seg, tm.p);
+        std::vector<double> h(J);
+        VG_CUDA(cudaMemcpyAsync(h.data(), tm.p, sizeof(double) * J, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        vg_sync(ctx);
+        for (auto &x : h) x = 1.0 / x; // distCalcConstantForSecondTerm (louvain.cpp:2217)
+        VG_CUDA(cudaMemcpyAsync(jconst.p, h.data(), sizeof(double) * J, cudaMemcpyHostToDevice,
+                                ctx->stream));
+        vg_sync(ctx);
+    }
+    {
+        LaunchTimer lt(ctx);
+        k_init<<<grid, 256, 0, ctx->stream>>>(nv, vdeg.p, cdeg.p, csize.p, cupd.p, B0.p, B1.p, B2.p,
+                                              nullptr, nullptr, nullptr);
+    }
+    VG_CHECK_LAUNCH();
+    Buckets bk;
+    build_buckets(ctx, U, nullptr, 1, bk);
+    GlobalTable gt;
+    if (bk.maxdeg_global > 0) {
+        int64_t cap = 32;
+        while (cap < 2 * bk.maxdeg_global) cap <<= 1;
+        const int64_t n6 = bk.start[5] - bk.start[4];
+        gt.blocks = (int)std::min<int64_t>(n6, (int64_t)ctx->sm_count * 2);
+        gt.cap = cap;
+        gt.keys.alloc(ctx, (size_t)cap * gt.blocks);
+        gt.vals.alloc(ctx, (size_t)cap * gt.blocks);
+    }
+    DevBuf<double> part(ctx, 3 * std::max<int64_t>(seg.C, 1));
+    const int agrid = seg_grid(ctx, seg.C);
+    // per-graph loop state
+    DevBuf<double> prev_mod(ctx, J), lower(ctx, J), thresh(ctx, J);
+    DevBuf<int32_t> iters(ctx, J), live(ctx, 1);
+    DevBuf<uint8_t> done(ctx, J);
+    DevBuf<int8_t> resbuf(ctx, J);
+    VG_CUDA(cudaMemcpyAsync(prev_mod.p, h_lower, sizeof(double) * J, cudaMemcpyHostToDevice, ctx->stream));
+    VG_CUDA(cudaMemcpyAsync(lower.p, h_lower, sizeof(double) * J, cudaMemcpyHostToDevice, ctx->stream));
+    VG_CUDA(cudaMemcpyAsync(thresh.p, h_thresh, sizeof(double) * J, cudaMemcpyHostToDevice, ctx->stream));
+    VG_CUDA(cudaMemsetAsync(iters.p, 0, sizeof(int32_t) * J, ctx->stream));
+    VG_CUDA(cudaMemsetAsync(done.p, 0, J, ctx->stream));
+    VG_CUDA(cudaMemsetAsync(resbuf.p, 0, J, ctx->stream));
+    int32_t *hlive = (int32_t *)vg_pinned(ctx, sizeof(int32_t));
+    int32_t *bufs[3] = {B0.p, B1.p, B2.p};
+    int pi = 0; // bufs[pi] = past, bufs[pi+1] = curr, bufs[pi+2] = target
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (sweep_ms) {
+        VG_CUDA(cudaEventCreate(&ev0));
+        VG_CUDA(cudaEventCreate(&ev1));
+        *sweep_ms = 0.0;
+    }
+    for (int32_t it = 1;; it++) {
+        SweepArgs a{};
+        a.rowptr = U->rowptr;
+        a.tail = U->tail;
+        a.weight = U->weight;
+        a.curr = bufs[(pi + 1) % 3];
+        a.target = bufs[(pi + 2) % 3];
+        a.vdeg = vdeg.p;
+        a.cdeg = cdeg.p;
+        a.csize = csize.p;
+        a.cupd = cupd.p;
+        a.cw = cw.p;
+        a.ref = U->ref;
+        a.ne = U->ne;
+        a.constant = 0.0;
+        a.vjob = vjob;
+        a.jconst = jconst.p;
+        a.jdone = done.p;
+        VG_CUDA(cudaMemsetAsync(live.p, 0, sizeof(int32_t), ctx->stream));
+        if (ev0) VG_CUDA(cudaEventRecord(ev0, ctx->stream));
+        sweep_color(ctx, a, bk, 0, gt, true, nv);
+        if (ev1) VG_CUDA(cudaEventRecord(ev1, ctx->stream));
+        {
+            LaunchTimer lt(ctx);
+            k_apply_seg<<<agrid, SEG_THREADS, 0, ctx->stream>>>(seg.voff.p, seg.cb.p, J, seg.C,
+                                                                cdeg.p, csize.p, cupd.p, cw.p,
+                                                                nullptr, done.p, 1, part.p);
+        }
+        VG_CHECK_LAUNCH();
+        BatchDecide bd;
+        bd.prev_mod = prev_mod.p;
+        bd.lower = lower.p;
+        bd.thresh = thresh.p;
+        bd.iters = iters.p;
+        bd.done = done.p;
+        bd.resbuf = resbuf.p;
+        bd.live_count = live.p;
+        bd.iter = it;
+        bd.past_idx = pi;
+        {
+            LaunchTimer lt(ctx);
+            k_mod_seg<<<(int)std::min<int64_t>(J, 65535), SEG_FINAL, 0, ctx->stream>>>(
+                part.p, seg.cb.p, J, 0.0, jconst.p, nullptr, bd);
+        }
+        VG_CHECK_LAUNCH();
+        VG_CUDA(cudaMemcpyAsync(hlive, live.p, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        vg_sync(ctx);
+        if (ev0) {
+            float ms = 0.f;
+            VG_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+            *sweep_ms += ms;
+        }
+        if (*hlive == 0) break;
+        pi = (pi + 1) % 3; // past <- curr <- target <- past (louvain.cpp:565-570)
+    }
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    vg_free(ctx, U->comm, sizeof(int32_t) * nv);
+    U->comm = nullptr;
+    DevBuf<int32_t> out(ctx, nv);
+    {
+        LaunchTimer lt(ctx);
+        k_gather_result<<<grid, 256, 0, ctx->stream>>>(nv, vjob, resbuf.p, B0.p, B1.p, B2.p, out.p);
+    }
+    VG_CHECK_LAUNCH();
+    U->comm = out.detach();
+    VG_CUDA(cudaMemcpyAsync(mod_out, prev_mod.p, sizeof(double) * J, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    VG_CUDA(cudaMemcpyAsync(iters_out, iters.p, sizeof(int32_t) * J, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    vg_sync(ctx);
 }
 
 void vg_phase_internal(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double *mod_out,
@@ -1292,7 +1634,7 @@ extern "C" vg_status vg_vertex_degree(vg_ctx *ctx, vg_graph *g, double *vdeg_out
                                                                          vdeg.p);
         }
         VG_CHECK_LAUNCH();
-        const double tm = g->nv ? vg_sum_f64(ctx, vdeg.p, g->nv) : 0.0;
+        const double tm = g->nv ? twice_m_one(ctx, vdeg.p, g->nv) : 0.0;
         if (constant_out) *constant_out = 1.0 / tm;
         if (vdeg_out && g->nv) {
             VG_CUDA(cudaMemcpyAsync(vdeg_out, vdeg.p, sizeof(double) * g->nv, cudaMemcpyDeviceToHost,
