@@ -39,6 +39,21 @@ METRIC = "Louvain e2e sec (RGG 2^24 +1% extra edges, full multi-level)"
 UNIT = "s"
 
 
+# batched workload: many small uneven graphs in one batch
+BATCH_GRAPHS = 4096
+BATCH_N = (1_000, 256_000)        # vertices, log-uniform
+BATCH_SEED = 4242
+BATCH_PLAIN_EVERY = 8             # plain path timed on every 8th graph
+BATCH_RESERVE = 80 << 30          # device pool mapped before the timed batch
+# served workload: Poisson stream of RGG / BA requests
+SERVE_REQUESTS = 96
+SERVE_E = (1e3, 5e7)              # CSR entries, log-uniform
+SERVE_SEED = 5151
+SERVE_LOAD = 8.0                  # offered load in units of the plain path's capacity
+SERVE_BUDGET = 48 << 30           # device-memory budget of the serving batch
+REL_TOL = 1e-9
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -47,6 +62,10 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_VERTICES, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu-baseline", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--batch-graphs", type=int, default=BATCH_GRAPHS, help=argparse.SUPPRESS)
+    ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS, help=argparse.SUPPRESS)
+    ap.add_argument("--skip-batched", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--skip-serving", action="store_true", help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -185,6 +204,169 @@ def run_reference_arm(args, rank: int, ws: int) -> None:
 
 
 # ---------------------------------------------------------------------------------------
+# batched and served forms
+
+
+def levels_agree(a: list, b: list) -> bool:
+    """Same levels (vertices, entries) and per-level modularity within REL_TOL."""
+    if len(a) != len(b):
+        return False
+    for x, y in zip(a, b):
+        if (x["nv"], x["ne"]) != (y["nv"], y["ne"]):
+            return False
+        if abs(x["modularity"] - y["modularity"]) > REL_TOL * abs(y["modularity"]):
+            return False
+    return True
+
+
+def batched_workload(ctx, count: int, seed: int):
+    """count graphs, n log-uniform in BATCH_N, half RGG (Vite's radius) and half
+    Erdos-Renyi (average degree 16), unit or U(0,1) weights per graph."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(BATCH_N[0]), np.log(BATCH_N[1]), count)).astype(np.int64)
+    kinds = rng.permutation(np.arange(count) % 2)
+    real = rng.integers(0, 2, count)
+    graphs = []
+    for i in range(count):
+        if kinds[i] == 0:
+            g = ctx.generate_rgg(int(ns[i]), 0.0, 0)
+        else:
+            g = ctx.generate_er(int(ns[i]), 16.0, seed * 100_003 + i)
+        if real[i]:
+            ctx.reweight(g, 2, seed * 7_919 + i)
+        else:
+            ctx.reweight(g, 1)
+        graphs.append(g)
+    return graphs, kinds, real
+
+
+def run_batched(ctx, stream, count: int) -> dict:
+    import torch
+
+    t0 = time.perf_counter()
+    graphs, kinds, real = batched_workload(ctx, count, BATCH_SEED)
+    gen_s = time.perf_counter() - t0
+    nv = [g.nv for g in graphs]
+    ne = [g.ne for g in graphs]
+    # warm-up of both paths on a few small graphs
+    warm = [ctx.generate_er(2000, 16.0, 1), ctx.generate_rgg(3000, 0.0, 0)]
+    for g in warm:
+        ctx.run(g, threshold=THRESHOLD)
+    ctx.run_batch(warm, threshold=THRESHOLD)
+    for g in warm:
+        g.free()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1) * 1e-3
+
+    sample = list(range(0, count, BATCH_PLAIN_EVERY))
+    plain, t_plain = timed(lambda: [ctx.run(graphs[i], threshold=THRESHOLD).stats for i in sample])
+    # the batch's working set is mapped once, as a long-running service would
+    ctx.reserve(min(40 * sum(ne) + 200 * sum(nv), BATCH_RESERVE))
+
+    def batch_all():
+        with ctx.batch() as b:
+            ids = [b.submit(g, threshold=THRESHOLD, take=True) for g in graphs]
+            b.run_all()
+            return [b.result(j).stats for j in ids], b.stats()
+
+    (res, bst), t_batch = timed(batch_all)
+    agree = sum(levels_agree(res[i], plain[k]) for k, i in enumerate(sample))
+    gps = count / t_batch
+    plain_gps = len(sample) / t_plain
+    return {
+        "workload": f"{count} graphs, n log-uniform [{BATCH_N[0]}, {BATCH_N[1]}], half RGG "
+                    f"(Vite radius) half Erdos-Renyi (avg degree 16), unit or U(0,1) FP64 "
+                    f"weights per graph, seed {BATCH_SEED}; full multi-level Louvain, "
+                    f"threshold {THRESHOLD:g}",
+        "graphs": count, "vertices": int(sum(nv)), "csr_entries": int(sum(ne)),
+        "rgg": int((kinds == 0).sum()), "real_weights": int(real.sum()),
+        "graphs_per_s": gps, "seconds": t_batch, "rounds": bst["rounds"],
+        "plain_graphs_per_s": plain_gps,
+        "plain_sample": f"every {BATCH_PLAIN_EVERY}th graph ({len(sample)} graphs) run alone "
+                        f"through vg_louvain_run back to back: {t_plain:.3f} s",
+        "speedup_vs_plain": gps / plain_gps,
+        "agree_with_plain": f"{agree}/{len(sample)} graphs: same levels, per-level modularity "
+                            f"within {REL_TOL:g} relative",
+        "generate_seconds": gen_s,
+    }
+
+
+def rgg_vertices_for_entries(e: float) -> int:
+    """n whose Vite-radius RGG has about e CSR entries (n * pi r(n)^2 * n)."""
+    def entries(n):
+        r = (np.sqrt(np.log(n) / (3.14159 * n)) + np.sqrt(2.0736 / n)) / 2.0
+        return n * 3.14159 * r * r * n
+    lo, hi = 16.0, 1e9
+    for _ in range(80):
+        mid = np.sqrt(lo * hi)
+        if entries(mid) < e:
+            lo = mid
+        else:
+            hi = mid
+    return int(round(lo))
+
+
+def serving_workload(ctx, count: int, seed: int):
+    """count requests, CSR entries log-uniform in SERVE_E, RGG (distance weights) or
+    Barabasi-Albert (m = 8, U(0,1) weights), unit-rate Poisson arrival times."""
+    rng = np.random.default_rng(seed)
+    es = np.exp(rng.uniform(np.log(SERVE_E[0]), np.log(SERVE_E[1]), count))
+    kinds = rng.integers(0, 2, count)
+    base = np.cumsum(rng.exponential(1.0, count))
+    graphs = []
+    for i in range(count):
+        if kinds[i] == 0:
+            g = ctx.generate_rgg(max(rgg_vertices_for_entries(es[i]), 64), 0.0, 0)
+        else:
+            g = ctx.generate_ba(max(int(es[i] / 16), 32), 8, seed * 1_000 + i)
+            ctx.reweight(g, 2, seed * 31 + i)
+        graphs.append(g)
+    return graphs, kinds, base
+
+
+def run_serving(ctx, count: int) -> dict:
+    from vite_b200 import serve as sv
+
+    graphs, kinds, base = serving_workload(ctx, count, SERVE_SEED)
+    ne = [g.ne for g in graphs]
+    reqs = [sv.Request(g, 0.0, THRESHOLD) for g in graphs]
+    plain = sv.sequential(ctx, reqs)
+    service = plain.stats["service_s"]
+    cap = count / sum(service)              # plain graphs/s, back to back
+    rate = SERVE_LOAD * cap
+    arrivals = base / base[-1] * (count / rate)
+    for r, a in zip(reqs, arrivals):
+        r.arrival = float(a)
+    fin = sv.fifo(arrivals, service)
+    plain_lat = fin - arrivals
+    ctx.reserve(SERVE_BUDGET)
+    served = sv.serve(ctx, reqs, budget=SERVE_BUDGET)
+    lat = served.latencies()
+    agree = sum(levels_agree(s.levels, p.levels) for s, p in zip(served.results, plain.results))
+    for g in graphs:
+        g.free()
+    return {
+        "workload": f"{count} requests, CSR entries log-uniform [{SERVE_E[0]:g}, {SERVE_E[1]:g}], "
+                    f"RGG (distance weights) or Barabasi-Albert m=8 (U(0,1) weights), Poisson "
+                    f"arrivals at {SERVE_LOAD:g}x the plain path's capacity, seed {SERVE_SEED}; "
+                    f"budget {SERVE_BUDGET >> 30} GiB; full multi-level Louvain",
+        "requests": count, "csr_entries": int(sum(ne)), "rate_per_s": rate,
+        "graphs_per_s": count / served.seconds, "p50_s": sv.percentile(lat, 50),
+        "p99_s": sv.percentile(lat, 99), "rounds": served.rounds,
+        "plain_graphs_per_s": count / float(fin.max() - arrivals.min()),
+        "plain_p50_s": sv.percentile(plain_lat, 50), "plain_p99_s": sv.percentile(plain_lat, 99),
+        "plain": "each request alone through vg_louvain_run, FIFO in arrival order (service "
+                 "times measured back to back on the device)",
+        "agree_with_plain": f"{agree}/{count} requests: same levels, per-level modularity within "
+                            f"{REL_TOL:g} relative",
+    }
 
 
 def main() -> None:
@@ -342,6 +524,10 @@ def main() -> None:
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    if ws == 1 and not args.skip_batched:
+        line["batched"] = run_batched(ctx, stream, args.batch_graphs)
+    if ws == 1 and not args.skip_serving:
+        line["serving"] = run_serving(ctx, args.serve_requests)
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.free()

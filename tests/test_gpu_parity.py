@@ -249,11 +249,16 @@ def test_rebuild_matches_oracle(ctx, maker):
 
 
 @pytest.mark.parametrize("layout", [0, 1])
-@pytest.mark.parametrize("case", ["one_community", "blocks_of_600", "random_blocks"])
+@pytest.mark.parametrize("case", ["one_community", "blocks_of_600", "random_blocks",
+                                  "ba_blocks_of_12"])
 def test_rebuild_segment_classes(ctx, case, layout):
-    """Next-level segments of every size class: warp (<=1024 entries), CTA (<=8192) and
-    the single-CTA global radix path (above), with real weights folded in order."""
-    if case == "one_community":
+    """Next-level segments of every size class: the warp hash path (<=256 entries, with
+    at most 32 or more distinct neighbours) and the global sorted path (longer), with
+    real weights folded in order."""
+    if case == "ba_blocks_of_12":
+        gref = vo.reweight(vo.ba(20000, 8, 6), 2, 11)
+        cv = (np.arange(gref.nv) // 12 * 12).astype(np.int64)
+    elif case == "one_community":
         gref = vo.reweight(star_graph(9000), 2, 5)
         cv = np.full(gref.nv, 17, np.int64)
     elif case == "blocks_of_600":

@@ -1,0 +1,41 @@
+"""The serving loop (vite_b200.serve): requests that arrive while others run join the
+running batch, finished ones are handed back and dropped, and every request's
+result is the one it gets alone (vg_louvain_run)."""
+import numpy as np
+import pytest
+
+from vite_b200 import serve as sv
+
+pytestmark = pytest.mark.gpu
+
+
+def test_fifo_finish_times():
+    fin = sv.fifo([0.0, 0.1, 5.0], [1.0, 1.0, 1.0])
+    assert list(fin) == [1.0, 2.0, 6.0]
+
+
+def test_served_results_equal_alone(ctx):
+    gs = []
+    for k in range(10):
+        if k % 2:
+            g = ctx.generate_ba(500 + 300 * k, 4, 100 + k)
+        else:
+            g = ctx.generate_rgg(800 + 900 * k, 0.0, 0)
+            ctx.reweight(g, 1)
+        gs.append(g)
+    alone = [ctx.run(g, want_comm=True) for g in gs]
+    # arrivals spread over a few rounds, so later requests join a running batch
+    reqs = [sv.Request(g, arrival=0.002 * k, want_comm=True) for k, g in enumerate(gs)]
+    rep = sv.serve(ctx, reqs, budget=1 << 30)
+    assert [r.index for r in rep.results] == list(range(len(gs)))
+    for r, a in zip(rep.results, alone):
+        assert r.latency >= 0.0
+        assert [(x["nv"], x["ne"], x["iters"], x["modularity"]) for x in r.levels] == \
+               [(x["nv"], x["ne"], x["iters"], x["modularity"]) for x in a.stats]
+        assert np.array_equal(r.comm, a.comm)
+    assert rep.stats["completed"] == len(gs)
+    seq = sv.sequential(ctx, reqs)
+    for r, a in zip(seq.results, alone):
+        assert [x["modularity"] for x in r.levels] == [x["modularity"] for x in a.stats]
+    for g in gs:
+        g.free()

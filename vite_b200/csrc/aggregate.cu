@@ -6,11 +6,10 @@
 //      (keys in reference order), so each row's entries can be copied as whole
 //      CSR rows, in the reference's (vertex, edge) order, into one segment;
 //   2. each segment is reduced by c2 with every sum a left fold in segment order,
-//      giving the reference's sums bit for bit: one thread per segment keeps up to
-//      16 distinct c2 in registers and sorts them with a network; segments with
-//      more distinct neighbours (or longer than 4096 entries) are sorted by c2
-//      (stable) -- one warp per segment up to 1024 entries, one CTA up to 8192, a
-//      single-CTA radix sort in global scratch above -- and their runs folded;
+//      giving the reference's sums bit for bit: one warp per segment of at most
+//      256 entries folds them into a shared-memory hash table in order and sorts
+//      the distinct keys; the longer segments go through one stable radix sort of
+//      all their entries by (segment, c2) and each run is folded in order;
 //   3. the unique entries are compacted into the next CSR.
 #include "vg_internal.cuh"
 
@@ -19,12 +18,6 @@
 
 namespace {
 
-constexpr int U_MAX = 16;     // thread path: distinct neighbours kept in registers
-constexpr int L_THREAD = 4096; // thread path: longest segment
-constexpr int W_MAX = 1024;   // warp path
-constexpr int C_MAX = 8192;   // CTA path
-constexpr int AG_WARPS = 8;
-constexpr int AG_THREADS = 256;
 
 __device__ __forceinline__ int32_t pos_of(const int32_t *__restrict__ pos, int64_t r) {
     return pos ? pos[r] : (int32_t)r;
@@ -97,298 +90,245 @@ __device__ void bitonic(uint64_t *sk, int n2, int t, int nt) {
         }
 }
 
-// fold the run that starts at sorted index i (keys packed key<<32 | index in segment)
-__device__ __forceinline__ double fold_run(const uint64_t *sk, int i, int L, const double *__restrict__ seg_w) {
-    const uint32_t key = (uint32_t)(sk[i] >> 32);
-    double s = seg_w[(uint32_t)sk[i]];
-    for (int j = i + 1; j < L && (uint32_t)(sk[j] >> 32) == key; j++) s = __dadd_rn(s, seg_w[(uint32_t)sk[j]]);
-    return s;
-}
+// One warp per segment of at most H_MAXL entries. The segment is read in chunks of
+// 32 entries; inside a chunk the lanes holding the same key elect the lowest as
+// leader, which adds its peers' weights in lane order onto the key's running sum
+// in a shared-memory table, so every sum is the left fold in segment order. Only
+// the distinct keys are then sorted: in registers across the warp when there are
+// at most 32 of them, else in shared memory. Longer segments are flagged.
+constexpr int H_MAXL = 256;
+constexpr int H_CAP = 512;
+constexpr int H_WARPS = 8;
+constexpr int32_t H_EMPTY = -1;
 
-// One thread per segment: entries are scanned in order and each is added to its
-// key's accumulator (a list of at most U_MAX keys in registers), so every sum is
-// the left fold in segment order; the list is then sorted by key with a
-// sorting network. Segments that are longer than L_THREAD or have more distinct
-// keys are flagged for the sorting paths below.
-__global__ void __launch_bounds__(256) k_rows_thread(
+struct HashWarpSmem {
+    int32_t keys[H_CAP];
+    double vals[H_CAP];
+    uint64_t list[H_MAXL]; // (key << 32 | slot) of the distinct keys
+    double stage[32];
+};
+
+__global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
     int64_t nc, const int64_t *__restrict__ rstart, const int32_t *__restrict__ gk,
     const double *__restrict__ gw, int32_t *__restrict__ uk, double *__restrict__ uw,
     int64_t *__restrict__ ucount, int32_t *__restrict__ flag) {
-    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < nc;
-         row += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t b = rstart[row];
-        const int64_t L = rstart[row + 1] - b;
-        if (L > L_THREAD) {
-            flag[row] = 1;
-            continue;
-        }
-        int32_t key[U_MAX];
-        double acc[U_MAX];
-#pragma unroll
-        for (int q = 0; q < U_MAX; q++) {
-            key[q] = INT_MAX;
-            acc[q] = 0.0;
-        }
-        int U = 0;
-        bool over = false;
-        for (int64_t i = 0; i < L; i++) {
-            const int32_t k = gk[b + i];
-            const double w = gw[b + i];
-            bool hit = false;
-#pragma unroll
-            for (int q = 0; q < U_MAX; q++)
-                if (q < U && key[q] == k) {
-                    acc[q] = __dadd_rn(acc[q], w);
-                    hit = true;
-                }
-            if (!hit) {
-                if (U == U_MAX) {
-                    over = true;
-                    break;
-                }
-#pragma unroll
-                for (int q = 0; q < U_MAX; q++)
-                    if (q == U) {
-                        key[q] = k;
-                        acc[q] = w;
-                    }
-                U++;
-            }
-        }
-        if (over) {
-            flag[row] = 1;
-            continue;
-        }
-        // bitonic network over the 16 (key, sum) pairs; unused slots hold INT_MAX
-#pragma unroll
-        for (int k2 = 2; k2 <= U_MAX; k2 <<= 1)
-#pragma unroll
-            for (int j = k2 >> 1; j > 0; j >>= 1)
-#pragma unroll
-                for (int i = 0; i < U_MAX; i++) {
-                    const int ixj = i ^ j;
-                    if (ixj > i) {
-                        const bool up = (i & k2) == 0;
-                        if ((key[i] > key[ixj]) == up) {
-                            const int32_t tk = key[i];
-                            key[i] = key[ixj];
-                            key[ixj] = tk;
-                            const double ta = acc[i];
-                            acc[i] = acc[ixj];
-                            acc[ixj] = ta;
-                        }
-                    }
-                }
-#pragma unroll
-        for (int q = 0; q < U_MAX; q++)
-            if (q < U) {
-                uk[b + q] = key[q];
-                uw[b + q] = acc[q];
-            }
-        ucount[row] = U;
-        flag[row] = 0;
-    }
-}
-
-__global__ void __launch_bounds__(AG_WARPS * 32) k_rows_warp(
-    int64_t nc, const int64_t *__restrict__ rstart, const int32_t *__restrict__ gk,
-    const double *__restrict__ gw, int32_t *__restrict__ uk, double *__restrict__ uw,
-    int64_t *__restrict__ ucount, const int32_t *__restrict__ flag) {
-    extern __shared__ uint64_t smem64[];
+    extern __shared__ unsigned char hsm_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t *sk = smem64 + (size_t)warp * W_MAX;
+    HashWarpSmem &S = reinterpret_cast<HashWarpSmem *>(hsm_raw)[warp];
+    const unsigned full = 0xffffffffu, lt = (1u << lane) - 1u;
     const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const unsigned lt = (1u << lane) - 1u;
     for (int64_t row = wg; row < nc; row += nw) {
-        if (!flag[row]) continue;
         const int64_t b = rstart[row];
-        const int L = (int)(rstart[row + 1] - b);
-        if (L > W_MAX) continue;
-        int n2 = 1;
-        while (n2 < L) n2 <<= 1;
-        for (int i = lane; i < n2; i += 32)
-            sk[i] = i < L ? (((uint64_t)(uint32_t)gk[b + i] << 32) | (uint32_t)i) : ~0ULL;
+        const int64_t L64 = rstart[row + 1] - b;
+        if (L64 > H_MAXL) {
+            if (lane == 0) flag[row] = 1;
+            continue;
+        }
+        const int L = (int)L64;
+        int logcap = 5;
+        while ((1 << logcap) < 2 * L) logcap++;
+        const int cap = 1 << logcap;
+        for (int s = lane; s < cap; s += 32) S.keys[s] = H_EMPTY;
         __syncwarp();
-        bitonic<true>(sk, n2, lane, 32);
-        int64_t u = 0;
+        int U = 0;
         for (int base = 0; base < L; base += 32) {
             const int i = base + lane;
-            const bool head = i < L && (i == 0 || (sk[i] >> 32) != (sk[i - 1] >> 32));
-            const unsigned hm = __ballot_sync(0xffffffffu, head);
-            if (head) {
-                const int64_t o = b + u + __popc(hm & lt);
-                uk[o] = (int32_t)(sk[i] >> 32);
-                uw[o] = fold_run(sk, i, L, gw + b);
+            const bool has = i < L;
+            int32_t k = -2 - lane; // distinct non-keys for idle lanes
+            double w = 0.0;
+            if (has) {
+                k = gk[b + i];
+                w = gw[b + i];
             }
-            u += __popc(hm);
+            S.stage[lane] = w;
+            const unsigned peers = __match_any_sync(full, k);
+            __syncwarp();
+            bool fresh = false;
+            int slot = 0;
+            if (has && lane == __ffs(peers) - 1) {
+                uint32_t h = ((uint32_t)k * 2654435761u) >> (32 - logcap);
+                for (;;) {
+                    const int32_t kk = S.keys[h];
+                    if (kk == k) break;
+                    if (kk == H_EMPTY) {
+                        const int32_t old = atomicCAS(&S.keys[h], H_EMPTY, k);
+                        if (old == H_EMPTY) {
+                            fresh = true;
+                            break;
+                        }
+                        if (old == k) break;
+                    }
+                    h = (h + 1) & (uint32_t)(cap - 1);
+                }
+                slot = (int)h;
+                double acc = fresh ? w : __dadd_rn(S.vals[h], w);
+                unsigned m = peers & (peers - 1);
+                while (m) {
+                    const int q = __ffs(m) - 1;
+                    acc = __dadd_rn(acc, S.stage[q]);
+                    m &= m - 1;
+                }
+                S.vals[h] = acc;
+            }
+            const unsigned fm = __ballot_sync(full, fresh);
+            if (fresh) S.list[U + __popc(fm & lt)] = ((uint64_t)(uint32_t)k << 32) | (uint32_t)slot;
+            U += __popc(fm);
+            __syncwarp();
         }
-        if (lane == 0) ucount[row] = u;
+        if (U <= 32) {
+            // bitonic network across the lanes on (key, sum)
+            int32_t key = INT_MAX;
+            double val = 0.0;
+            if (lane < U) {
+                const uint64_t e = S.list[lane];
+                key = (int32_t)(e >> 32);
+                val = S.vals[(uint32_t)e];
+            }
+#pragma unroll
+            for (int k2 = 2; k2 <= 32; k2 <<= 1)
+#pragma unroll
+                for (int j = k2 >> 1; j > 0; j >>= 1) {
+                    const int32_t pk = __shfl_xor_sync(full, key, j);
+                    const double pv = __shfl_xor_sync(full, val, j);
+                    const bool up = (lane & k2) == 0;
+                    const bool low = (lane & j) == 0;
+                    // the lower lane of an ascending pair keeps the minimum
+                    const bool take = (low == up) ? (pk < key) : (pk > key);
+                    if (take) {
+                        key = pk;
+                        val = pv;
+                    }
+                }
+            if (lane < U) {
+                uk[b + lane] = key;
+                uw[b + lane] = val;
+            }
+        } else {
+            int n2 = 64;
+            while (n2 < U) n2 <<= 1;
+            for (int i = U + lane; i < n2; i += 32) S.list[i] = ~0ULL;
+            __syncwarp();
+            bitonic<true>(S.list, n2, lane, 32);
+            for (int i = lane; i < U; i += 32) {
+                const uint64_t e = S.list[i];
+                uk[b + i] = (int32_t)(e >> 32);
+                uw[b + i] = S.vals[(uint32_t)e];
+            }
+        }
+        if (lane == 0) {
+            ucount[row] = U;
+            flag[row] = 0;
+        }
         __syncwarp();
     }
 }
 
-// block-wide exclusive scan of one int per thread (AG_THREADS threads)
-__device__ int block_scan_excl(int v, int *total, int *ws) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int x = v;
+// Segments longer than H_MAXL, all together: every entry becomes the key
+// (segment rank << kbits | neighbour key) with its index in the grouped arrays as
+// payload; one stable radix sort over all of them puts each (segment, key) run in
+// segment order, and the run is folded left to right.
+__global__ void k_big_rowmap(int64_t nc, const int32_t *__restrict__ flag,
+                             const int64_t *__restrict__ bigidx, int32_t *__restrict__ big_row) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nc;
+         r += (int64_t)gridDim.x * blockDim.x)
+        if (flag[r]) big_row[bigidx[r]] = (int32_t)r;
+}
+
+__global__ void k_big_lengths(int64_t nc, const int32_t *__restrict__ flag,
+                              const int64_t *__restrict__ rstart, int64_t *__restrict__ len) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nc;
+         r += (int64_t)gridDim.x * blockDim.x)
+        len[r] = flag[r] ? rstart[r + 1] - rstart[r] : 0;
+}
+
+constexpr int BIG_CHUNK = 4096;
+
+__global__ void k_big_chunks(int64_t nbig, const int32_t *__restrict__ big_row,
+                             const int64_t *__restrict__ rstart, int64_t *__restrict__ nch) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nbig;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t r = big_row[q];
+        nch[q] = (rstart[r + 1] - rstart[r] + BIG_CHUNK - 1) / BIG_CHUNK;
+    }
+}
+
+// one block per chunk of BIG_CHUNK entries of a long segment
+__global__ void k_big_keys(int64_t nbig, const int64_t *__restrict__ cb, int64_t nchunks,
+                           const int32_t *__restrict__ big_row, const int64_t *__restrict__ rstart,
+                           const int64_t *__restrict__ boff, const int32_t *__restrict__ gk,
+                           int kbits, uint64_t *__restrict__ K, uint32_t *__restrict__ V) {
+    for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        int64_t lo = 0, hi = nbig; // largest q with cb[q] <= c
+        while (hi - lo > 1) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (cb[mid] <= c) lo = mid;
+            else hi = mid;
+        }
+        const int64_t q = lo;
+        const int32_t r = big_row[q];
+        const int64_t b = rstart[r], L = rstart[r + 1] - b, o = boff[r];
+        const int64_t i0 = (c - cb[q]) * BIG_CHUNK, i1 = min(i0 + BIG_CHUNK, L);
+        for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+            K[o + i] = ((uint64_t)q << kbits) | (uint64_t)(uint32_t)gk[b + i];
+            V[o + i] = (uint32_t)(b + i);
+        }
+    }
+}
+
+__global__ void k_big_heads(const uint64_t *__restrict__ K, int64_t m, int32_t *__restrict__ h) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x)
+        h[i] = (i == 0 || K[i] != K[i - 1]) ? 1 : 0;
+}
+
+__global__ void k_big_rowfirst(const uint64_t *__restrict__ K, int64_t m, int kbits,
+                               const int64_t *__restrict__ hr, int64_t *__restrict__ rowfirst,
+                               int64_t *__restrict__ headpos) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = K[i];
+        const uint64_t q = k >> kbits;
+        if (i == 0 || (K[i - 1] >> kbits) != q) rowfirst[q] = hr[i];
+        if (i == 0 || K[i - 1] != k) headpos[hr[i]] = i;
+    }
+}
+
+// one thread per run: the run's bounds are known, so its weights are fetched
+// eight at a time ahead of the strictly ordered additions
+__global__ void k_big_fold(const uint64_t *__restrict__ K, const uint32_t *__restrict__ V, int64_t m,
+                           int kbits, int64_t nheads, const int64_t *__restrict__ headpos,
+                           const int64_t *__restrict__ rowfirst, const int32_t *__restrict__ big_row,
+                           const int64_t *__restrict__ rstart, const double *__restrict__ gw,
+                           int32_t *__restrict__ uk, double *__restrict__ uw) {
+    const uint64_t mask = ((uint64_t)1 << kbits) - 1;
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nheads;
+         h += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i0 = headpos[h], i1 = h + 1 < nheads ? headpos[h + 1] : m;
+        const uint64_t k = K[i0];
+        const uint64_t q = k >> kbits;
+        double s = gw[V[i0]];
+        int64_t j = i0 + 1;
+        for (; j + 8 <= i1; j += 8) {
+            double x[8];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) ws[warp] = x;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int w = 0; w < AG_THREADS / 32; w++) {
-            const int c = ws[w];
-            ws[w] = run;
-            run += c;
+            for (int t = 0; t < 8; t++) x[t] = gw[V[j + t]];
+#pragma unroll
+            for (int t = 0; t < 8; t++) s = __dadd_rn(s, x[t]);
         }
-        ws[AG_THREADS / 32] = run;
-    }
-    __syncthreads();
-    const int r = ws[warp] + x - v;
-    *total = ws[AG_THREADS / 32];
-    __syncthreads();
-    return r;
-}
-
-// fold + compaction of a sorted segment by a whole CTA
-__device__ void cta_fold(const uint64_t *sk, int L, int64_t b, const double *__restrict__ gw,
-                         int32_t *__restrict__ uk, double *__restrict__ uw, int64_t *ucount_row,
-                         int *ws) {
-    int64_t u = 0;
-    for (int base = 0; base < L; base += AG_THREADS) {
-        const int i = base + threadIdx.x;
-        const bool head = i < L && (i == 0 || (sk[i] >> 32) != (sk[i - 1] >> 32));
-        int tot;
-        const int rank = block_scan_excl(head ? 1 : 0, &tot, ws);
-        if (head) {
-            const int64_t o = b + u + rank;
-            uk[o] = (int32_t)(sk[i] >> 32);
-            uw[o] = fold_run(sk, i, L, gw + b);
-        }
-        u += tot;
-    }
-    if (threadIdx.x == 0) *ucount_row = u;
-}
-
-__global__ void __launch_bounds__(AG_THREADS) k_rows_cta(
-    int64_t nc, const int64_t *__restrict__ rstart, const int32_t *__restrict__ gk,
-    const double *__restrict__ gw, int32_t *__restrict__ uk, double *__restrict__ uw,
-    int64_t *__restrict__ ucount, const int32_t *__restrict__ flag) {
-    extern __shared__ uint64_t smem64[];
-    __shared__ int ws[AG_THREADS / 32 + 1];
-    for (int64_t row = blockIdx.x; row < nc; row += gridDim.x) {
-        if (!flag[row]) continue;
-        const int64_t b = rstart[row];
-        const int L = (int)(rstart[row + 1] - b);
-        if (L <= W_MAX || L > C_MAX) continue;
-        int n2 = 1;
-        while (n2 < L) n2 <<= 1;
-        for (int i = threadIdx.x; i < n2; i += AG_THREADS)
-            smem64[i] = i < L ? (((uint64_t)(uint32_t)gk[b + i] << 32) | (uint32_t)i) : ~0ULL;
-        __syncthreads();
-        bitonic<false>(smem64, n2, threadIdx.x, AG_THREADS);
-        cta_fold(smem64, L, b, gw, uk, uw, ucount + row, ws);
-        __syncthreads();
+        for (; j < i1; j++) s = __dadd_rn(s, gw[V[j]]);
+        const int64_t o = rstart[big_row[q]] + (h - rowfirst[q]);
+        uk[o] = (int32_t)(k & mask);
+        uw[o] = s;
     }
 }
 
-// segments above C_MAX: a single-CTA stable LSD radix sort in global scratch
-// (scratch holds 2*L packed keys per segment, at offset sbase[row])
-__global__ void __launch_bounds__(AG_THREADS) k_rows_big(
-    int64_t nc, const int64_t *__restrict__ rstart, const int32_t *__restrict__ gk,
-    const double *__restrict__ gw, int32_t *__restrict__ uk, double *__restrict__ uw,
-    int64_t *__restrict__ ucount, const int64_t *__restrict__ sbase, uint64_t *__restrict__ scratch,
-    int key_bits, const int32_t *__restrict__ flag) {
-    __shared__ int hist[256];
-    __shared__ int64_t dbase[256];
-    __shared__ int wcnt[AG_THREADS / 32][256];
-    __shared__ int ws[AG_THREADS / 32 + 1];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int64_t row = blockIdx.x; row < nc; row += gridDim.x) {
-        if (!flag[row]) continue;
-        const int64_t b = rstart[row];
-        const int64_t L = rstart[row + 1] - b;
-        if (L <= C_MAX) continue;
-        uint64_t *A = scratch + sbase[row], *B = A + L;
-        for (int64_t i = threadIdx.x; i < L; i += AG_THREADS)
-            A[i] = ((uint64_t)(uint32_t)gk[b + i] << 32) | (uint32_t)i;
-        __syncthreads();
-        for (int shift = 32; shift < 32 + key_bits; shift += 8) {
-            hist[threadIdx.x] = 0;
-            __syncthreads();
-            for (int64_t i = threadIdx.x; i < L; i += AG_THREADS) atomicAdd(&hist[(A[i] >> shift) & 0xff], 1);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                int64_t run = 0;
-                for (int d = 0; d < 256; d++) {
-                    dbase[d] = run;
-                    run += hist[d];
-                }
-            }
-            __syncthreads();
-            for (int64_t base = 0; base < L; base += AG_THREADS) {
-                for (int w = 0; w < AG_THREADS / 32; w++) wcnt[w][threadIdx.x] = 0;
-                __syncthreads();
-                const int64_t i = base + threadIdx.x;
-                const bool valid = i < L;
-                const uint64_t x = valid ? A[i] : 0;
-                const int d = valid ? (int)((x >> shift) & 0xff) : 256 + lane;
-                const unsigned peers = __match_any_sync(0xffffffffu, d);
-                const int rk = __popc(peers & lt);
-                if (valid && rk == 0) wcnt[warp][d] = __popc(peers);
-                __syncthreads();
-                int run = 0;
-                for (int w = 0; w < AG_THREADS / 32; w++) {
-                    const int c = wcnt[w][threadIdx.x];
-                    wcnt[w][threadIdx.x] = run;
-                    run += c;
-                }
-                __syncthreads();
-                if (valid) B[dbase[d] + wcnt[warp][d] + rk] = x;
-                __syncthreads();
-                dbase[threadIdx.x] += run;
-                __syncthreads();
-            }
-            uint64_t *t = A;
-            A = B;
-            B = t;
-            __syncthreads();
-        }
-        // fold from global scratch
-        int64_t u = 0;
-        for (int64_t base = 0; base < L; base += AG_THREADS) {
-            const int64_t i = base + threadIdx.x;
-            const bool head = i < L && (i == 0 || (A[i] >> 32) != (A[i - 1] >> 32));
-            int tot;
-            const int rank = block_scan_excl(head ? 1 : 0, &tot, ws);
-            if (head) {
-                const uint32_t key = (uint32_t)(A[i] >> 32);
-                double s = gw[b + (uint32_t)A[i]];
-                for (int64_t j = i + 1; j < L && (uint32_t)(A[j] >> 32) == key; j++)
-                    s = __dadd_rn(s, gw[b + (uint32_t)A[j]]);
-                uk[b + u + rank] = (int32_t)key;
-                uw[b + u + rank] = s;
-            }
-            u += tot;
-        }
-        if (threadIdx.x == 0) ucount[row] = u;
-        __syncthreads();
-    }
-}
-
-__global__ void k_big_sizes(int64_t nc, const int64_t *__restrict__ rstart,
-                            const int32_t *__restrict__ flag, int64_t *__restrict__ sz) {
-    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < nc;
-         row += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t L = rstart[row + 1] - rstart[row];
-        sz[row] = (flag[row] && L > C_MAX) ? 2 * L : 0;
-    }
+__global__ void k_big_counts(int64_t nbig, const int32_t *__restrict__ big_row,
+                             const int64_t *__restrict__ rowfirst, int64_t heads,
+                             int64_t *__restrict__ ucount) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nbig;
+         q += (int64_t)gridDim.x * blockDim.x)
+        ucount[big_row[q]] = (q + 1 < nbig ? rowfirst[q + 1] : heads) - rowfirst[q];
 }
 
 __global__ void k_compact_rows(int64_t nc, const int64_t *__restrict__ rstart,
@@ -420,10 +360,8 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     const int64_t nv = g->nv, ne = g->ne;
     static bool configured = false;
     if (!configured) {
-        VG_CUDA(cudaFuncSetAttribute(k_rows_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(AG_WARPS * W_MAX * sizeof(uint64_t))));
-        VG_CUDA(cudaFuncSetAttribute(k_rows_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(C_MAX * sizeof(uint64_t))));
+        VG_CUDA(cudaFuncSetAttribute(k_rows_hash, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(H_WARPS * sizeof(HashWarpSmem))));
         configured = true;
     }
     int kbits = 1;
@@ -473,32 +411,65 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     DevBuf<int32_t> flag(ctx, nc);
     if (nc) {
         { LaunchTimer lt(ctx);
-          k_rows_thread<<<vg_grid(ctx, nc, 256, 8), 256, 0, ctx->stream>>>(
+          k_rows_hash<<<vg_grid(ctx, nc * 32, H_WARPS * 32, 3), H_WARPS * 32,
+                        H_WARPS * sizeof(HashWarpSmem), ctx->stream>>>(
               nc, rstart.p, gk.p, gw.p, uk.p, uw.p, ucount.p, flag.p); }
         VG_CHECK_LAUNCH();
-        { LaunchTimer lt(ctx);
-          k_rows_warp<<<vg_grid(ctx, nc * 32, AG_WARPS * 32, 4), AG_WARPS * 32,
-                        AG_WARPS * W_MAX * sizeof(uint64_t), ctx->stream>>>(nc, rstart.p, gk.p, gw.p,
-                                                                            uk.p, uw.p, ucount.p, flag.p); }
-        VG_CHECK_LAUNCH();
-        { LaunchTimer lt(ctx);
-          k_rows_cta<<<vg_grid(ctx, nc, 1, 2), AG_THREADS, C_MAX * sizeof(uint64_t), ctx->stream>>>(
-              nc, rstart.p, gk.p, gw.p, uk.p, uw.p, ucount.p, flag.p); }
-        VG_CHECK_LAUNCH();
-        // big segments: scratch sized by their total length
-        DevBuf<int64_t> sbase(ctx, nc + 1);
-        VG_CUDA(cudaMemsetAsync(sbase.p + nc, 0, sizeof(int64_t), ctx->stream));
-        { LaunchTimer lt(ctx);
-          k_big_sizes<<<vg_grid(ctx, nc, 256), 256, 0, ctx->stream>>>(nc, rstart.p, flag.p, sbase.p); }
-        VG_CHECK_LAUNCH();
-        const int64_t big = vg_exclusive_scan_i64(ctx, sbase.p, nc + 1);
-        if (big > 0) {
-            DevBuf<uint64_t> scratch(ctx, big);
-            LaunchTimer lt(ctx);
-            k_rows_big<<<vg_grid(ctx, nc, 1, 2), AG_THREADS, 0, ctx->stream>>>(
-                nc, rstart.p, gk.p, gw.p, uk.p, uw.p, ucount.p, sbase.p, scratch.p, kbits, flag.p);
+        // segments longer than H_MAXL: one global stable sort
+        DevBuf<int64_t> bigidx(ctx, nc + 1), boff(ctx, nc + 1);
+        const int64_t nbig = vg_exclusive_scan_i32_to_i64(ctx, flag.p, bigidx.p, nc);
+        if (nbig > 0) {
+            { LaunchTimer lt(ctx);
+              k_big_lengths<<<vg_grid(ctx, nc, 256), 256, 0, ctx->stream>>>(nc, flag.p, rstart.p,
+                                                                            boff.p); }
             VG_CHECK_LAUNCH();
-            vg_sync(ctx);
+            const int64_t m = vg_exclusive_scan_i64(ctx, boff.p, nc);
+            DevBuf<int32_t> big_row(ctx, nbig);
+            { LaunchTimer lt(ctx);
+              k_big_rowmap<<<vg_grid(ctx, nc, 256), 256, 0, ctx->stream>>>(nc, flag.p, bigidx.p,
+                                                                           big_row.p); }
+            VG_CHECK_LAUNCH();
+            int qbits = 1;
+            while (qbits < 32 && ((int64_t)1 << qbits) < nbig) qbits++;
+            VG_REQUIRE(kbits + qbits <= 64, "aggregation keys need %d bits", kbits + qbits);
+            DevBuf<uint64_t> K(ctx, m);
+            DevBuf<uint32_t> V(ctx, m);
+            {
+                DevBuf<int64_t> cb(ctx, nbig + 1);
+                { LaunchTimer lt(ctx);
+                  k_big_chunks<<<vg_grid(ctx, nbig, 256), 256, 0, ctx->stream>>>(nbig, big_row.p,
+                                                                                rstart.p, cb.p); }
+                VG_CHECK_LAUNCH();
+                const int64_t nch = vg_exclusive_scan_i64(ctx, cb.p, nbig);
+                { LaunchTimer lt(ctx);
+                  k_big_keys<<<(int)std::min<int64_t>(nch, 16LL * ctx->sm_count), 256, 0,
+                               ctx->stream>>>(nbig, cb.p, nch, big_row.p, rstart.p, boff.p, gk.p,
+                                              kbits, K.p, V.p); }
+                VG_CHECK_LAUNCH();
+            }
+            vg_radix_sort_pairs(ctx, K.p, V.p, m, kbits + qbits);
+            DevBuf<int32_t> heads(ctx, m);
+            DevBuf<int64_t> hr(ctx, m), rowfirst(ctx, nbig);
+            { LaunchTimer lt(ctx);
+              k_big_heads<<<vg_grid(ctx, m, 256), 256, 0, ctx->stream>>>(K.p, m, heads.p); }
+            VG_CHECK_LAUNCH();
+            const int64_t nheads = vg_exclusive_scan_i32_to_i64(ctx, heads.p, hr.p, m);
+            heads.release();
+            DevBuf<int64_t> headpos(ctx, nheads);
+            { LaunchTimer lt(ctx);
+              k_big_rowfirst<<<vg_grid(ctx, m, 256), 256, 0, ctx->stream>>>(K.p, m, kbits, hr.p,
+                                                                            rowfirst.p, headpos.p); }
+            VG_CHECK_LAUNCH();
+            hr.release();
+            { LaunchTimer lt(ctx);
+              k_big_fold<<<vg_grid(ctx, nheads, 128), 128, 0, ctx->stream>>>(
+                  K.p, V.p, m, kbits, nheads, headpos.p, rowfirst.p, big_row.p, rstart.p, gw.p,
+                  uk.p, uw.p); }
+            VG_CHECK_LAUNCH();
+            { LaunchTimer lt(ctx);
+              k_big_counts<<<vg_grid(ctx, nbig, 256), 256, 0, ctx->stream>>>(
+                  nbig, big_row.p, rowfirst.p, nheads, ucount.p); }
+            VG_CHECK_LAUNCH();
         }
     }
     gk.release();

@@ -27,6 +27,7 @@ vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm);
 namespace {
 
 constexpr int PACK_VCHUNK = 2048;
+constexpr int64_t MAX_UNION = INT32_MAX; // vertices and CSR entries of one packed graph
 constexpr int PACK_ECHUNK = 8192;
 
 // one source range of a pack: vertices [v_lo, v_lo + nv) with edges
@@ -173,6 +174,7 @@ struct BJob {
     int64_t nv0 = 0, ne0 = 0;
     size_t est = 0;
     JobState state = QUEUED;
+    bool forgotten = false; // results dropped; erased once out of the packed graph
     // level loop (main.cpp:242-513)
     double prevMod = -1.0;
     int phase = 0, tot_iters = 0;
@@ -471,22 +473,43 @@ void check_params(const vg_run_params *rp) {
     VG_REQUIRE(rp->layout >= 0 && rp->layout <= 2, "layout must be 0, 1 or 2");
 }
 
+// erase the forgotten jobs that are no longer part of the packed graph
+void sweep_forgotten(vg_batch *b) {
+    std::vector<int64_t> gone;
+    for (auto &kv : b->jobs)
+        if (kv.second->forgotten &&
+            std::find(b->running.begin(), b->running.end(), kv.first) == b->running.end())
+            gone.push_back(kv.first);
+    for (int64_t id : gone) b->jobs.erase(id);
+}
+
 // one round: admit, phase, per-graph level bookkeeping, rebuild
 void step(vg_batch *b) {
     vg_ctx *ctx = b->ctx;
-    // admission: first come first served while the estimated footprint fits
+    std::vector<int64_t> keep;
+    int64_t union_nv = 0, union_ne = 0;
+    for (int64_t id : b->running) {
+        const BJob &j = *b->jobs.at(id);
+        if (j.state != RUNNING) continue;
+        keep.push_back(id);
+        union_nv += j.nv;
+        union_ne += j.ne;
+    }
+    // admission: first come first served while the estimated footprint fits the
+    // budget and the union stays within 32-bit vertex and edge indexing
     std::vector<int64_t> admit;
     size_t bytes = b->running_bytes;
     while (!b->queue.empty()) {
         BJob &j = *b->jobs.at(b->queue.front());
-        if (b->budget && bytes + j.est > b->budget && !(b->running.empty() && admit.empty())) break;
+        const bool alone = keep.empty() && admit.empty();
+        if (b->budget && bytes + j.est > b->budget && !alone) break;
+        if (union_nv + j.nv0 > MAX_UNION || union_ne + j.ne0 > MAX_UNION) break;
         bytes += j.est;
+        union_nv += j.nv0;
+        union_ne += j.ne0;
         admit.push_back(j.id);
         b->queue.pop_front();
     }
-    std::vector<int64_t> keep;
-    for (int64_t id : b->running)
-        if (b->jobs.at(id)->state == RUNNING) keep.push_back(id);
     if (keep.empty() && admit.empty()) {
         release_graph(ctx, b->U);
         b->vjob.release();
@@ -494,6 +517,7 @@ void step(vg_batch *b) {
         b->voff.assign(1, 0);
         b->eoff.assign(1, 0);
         b->dirty = false;
+        sweep_forgotten(b);
         return;
     }
     if (!admit.empty() || b->dirty || keep.size() != b->running.size()) {
@@ -505,6 +529,7 @@ void step(vg_batch *b) {
         }
         b->running_bytes = bytes;
         b->st.admitted += (int64_t)admit.size();
+        sweep_forgotten(b);
     }
     if (b->running.empty()) return;
     const int64_t J = (int64_t)b->running.size();
@@ -588,6 +613,7 @@ void step(vg_batch *b) {
         b->running.clear();
         b->voff.assign(1, 0);
         b->eoff.assign(1, 0);
+        sweep_forgotten(b);
     }
     b->st.rounds++;
     b->st.seconds_phase += phase_s;
@@ -635,6 +661,8 @@ extern "C" vg_status vg_batch_submit(vg_batch *b, vg_graph *g, const vg_run_para
     return vg_guard(b->ctx, [&] {
         check_params(rp);
         VG_REQUIRE(g->nv >= 1 && g->ne >= 1, "a batched graph needs vertices and edges");
+        VG_REQUIRE(g->nv <= MAX_UNION && g->ne <= MAX_UNION,
+                   "a batched graph has fewer than 2^31 vertices and CSR entries");
         auto j = std::make_unique<BJob>();
         j->id = b->next_id++;
         j->src = g;
@@ -682,7 +710,8 @@ extern "C" vg_status vg_batch_result(vg_batch *b, int64_t job, vg_level_stat *le
     if (!b) return VG_ERR_ARG;
     return vg_guard(b->ctx, [&] {
         auto it = b->jobs.find(job);
-        VG_REQUIRE(it != b->jobs.end(), "unknown batch job %lld", (long long)job);
+        VG_REQUIRE(it != b->jobs.end() && !it->second->forgotten, "unknown batch job %lld",
+                   (long long)job);
         BJob &j = *it->second;
         VG_REQUIRE(j.state == DONE, "batch job %lld has not finished", (long long)job);
         const int32_t n = (int32_t)j.stats.size();
@@ -710,10 +739,17 @@ extern "C" vg_status vg_batch_forget(vg_batch *b, int64_t job) {
     if (!b) return VG_ERR_ARG;
     return vg_guard(b->ctx, [&] {
         auto it = b->jobs.find(job);
-        VG_REQUIRE(it != b->jobs.end(), "unknown batch job %lld", (long long)job);
+        VG_REQUIRE(it != b->jobs.end() && !it->second->forgotten, "unknown batch job %lld",
+                   (long long)job);
         VG_REQUIRE(it->second->state == DONE, "batch job %lld has not finished", (long long)job);
         VG_CUDA(cudaSetDevice(b->ctx->device));
-        b->jobs.erase(it);
+        if (std::find(b->running.begin(), b->running.end(), job) == b->running.end()) {
+            b->jobs.erase(it);
+        } else { // still a range of the packed graph until the next step repacks it
+            it->second->forgotten = true;
+            it->second->all.release();
+            it->second->stats.clear();
+        }
     });
 }
 

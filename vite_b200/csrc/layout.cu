@@ -35,22 +35,49 @@ __global__ void k_bfs_init(int64_t nv, uint64_t seed, int32_t *__restrict__ labe
     }
 }
 
-// one level: vertices at distance step-1 claim their unlabeled neighbours
+// one level: vertices at distance step-1 claim their unlabeled neighbours. A warp
+// takes 32 consecutive vertices; a frontier row of at most 64 entries is scanned
+// by its own lane, a longer one by the whole warp.
+__device__ __forceinline__ unsigned long long bfs_claim(const int32_t *__restrict__ tail, int64_t e,
+                                                        int32_t lu, int step,
+                                                        int32_t *__restrict__ label,
+                                                        uint8_t *__restrict__ dist) {
+    const int32_t w = tail[e];
+    if (label[w] == -1 && atomicCAS(&label[w], -1, lu) == -1) {
+        dist[w] = (uint8_t)step;
+        return 1;
+    }
+    return 0;
+}
+
 __global__ void k_bfs_step(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
                            int64_t nv, int step, int32_t *__restrict__ label,
                            uint8_t *__restrict__ dist, unsigned long long *__restrict__ claimed) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long mine = 0;
-    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < nv;
-         u += (int64_t)gridDim.x * blockDim.x) {
-        if (dist[u] != step - 1) continue;
-        const int32_t lu = label[u];
-        const int64_t e1 = rowptr[u + 1];
-        for (int64_t e = rowptr[u]; e < e1; e++) {
-            const int32_t w = tail[e];
-            if (label[w] == -1 && atomicCAS(&label[w], -1, lu) == -1) {
-                dist[w] = (uint8_t)step;
-                mine++;
-            }
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < nv;
+         base += nw * 32) {
+        const int64_t u = base + lane;
+        const bool front = u < nv && dist[u] == step - 1;
+        int64_t e0 = 0, e1 = 0;
+        int32_t lu = -1;
+        if (front) {
+            e0 = rowptr[u];
+            e1 = rowptr[u + 1];
+            lu = label[u];
+        }
+        const bool lng = front && e1 - e0 > 64;
+        if (front && !lng)
+            for (int64_t e = e0; e < e1; e++) mine += bfs_claim(tail, e, lu, step, label, dist);
+        unsigned lm = __ballot_sync(full, lng);
+        while (lm) {
+            const int src = __ffs(lm) - 1;
+            lm &= lm - 1;
+            const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
+            const int32_t L = __shfl_sync(full, lu, src);
+            for (int64_t e = E0 + lane; e < E1; e += 32) mine += bfs_claim(tail, e, L, step, label, dist);
         }
     }
 #pragma unroll

@@ -711,15 +711,45 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
 // ---------------------------------------------------------------------------------
 // init, degree, apply + modularity, swaps
 
-// distSumVertexDegree (louvain.cpp:2161-2186): each row summed in CSR order
+// distSumVertexDegree (louvain.cpp:2161-2186): each row summed in CSR order. A
+// warp takes 32 consecutive rows; a row of at most DEG_LONG entries is summed by
+// its own lane, a longer one by the whole warp: coalesced loads of 32 entries,
+// added one after the other (every lane forms the same left fold).
+constexpr int DEG_LONG = 64;
+
 __global__ void k_degree(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
                          int64_t nv, double *__restrict__ vdeg) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        double tw = 0.0;
-        const int64_t e1 = rowptr[i + 1];
-        for (int64_t k = rowptr[i]; k < e1; k++) tw = __dadd_rn(tw, w[k]);
-        vdeg[i] = tw;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < nv;
+         base += nw * 32) {
+        const int64_t v = base + lane;
+        const bool valid = v < nv;
+        int64_t e0 = 0, e1 = 0;
+        if (valid) {
+            e0 = rowptr[v];
+            e1 = rowptr[v + 1];
+        }
+        const bool lng = valid && e1 - e0 > DEG_LONG;
+        if (valid && !lng) {
+            double tw = 0.0;
+            for (int64_t k = e0; k < e1; k++) tw = __dadd_rn(tw, w[k]);
+            vdeg[v] = tw;
+        }
+        unsigned lm = __ballot_sync(full, lng);
+        while (lm) {
+            const int src = __ffs(lm) - 1;
+            lm &= lm - 1;
+            const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
+            double sum = 0.0;
+            for (int64_t off = E0; off < E1; off += 32) {
+                const double x = off + lane < E1 ? w[off + lane] : 0.0;
+                const int n = (int)min((int64_t)32, E1 - off);
+                for (int q = 0; q < n; q++) sum = __dadd_rn(sum, __shfl_sync(full, x, q));
+            }
+            if (lane == src) vdeg[v] = sum;
+        }
     }
 }
 

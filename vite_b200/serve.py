@@ -1,0 +1,139 @@
+"""Served Louvain: a request loop over one running batch (continuous batching).
+
+Requests (a device graph and its run parameters) arrive over time. Whenever the
+device is free between rounds, every request that has arrived is submitted to the
+batch; the batch admits what fits its device-memory budget, runs one round (one
+phase for every graph in it, then the rebuild), and the graphs whose level loop
+ended are handed back with their latency (finish time - arrival time). Work of
+requests that arrive while others run overlaps on the device in the same
+launches, and each result is the one a run of its own gives.
+
+``sequential`` is the plain path the batch is measured against: one
+vg_louvain_run per request in arrival order, a single FIFO server.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import Batch, Context, Graph
+
+
+@dataclass
+class Request:
+    graph: Graph
+    arrival: float              # seconds after the start of the stream
+    threshold: float = 1e-6
+    want_comm: bool = False
+
+
+@dataclass
+class Served:
+    index: int
+    arrival: float
+    finish: float
+    levels: list
+    comm: np.ndarray | None = None
+
+    @property
+    def latency(self) -> float:
+        return self.finish - self.arrival
+
+
+@dataclass
+class ServeReport:
+    results: list
+    seconds: float              # first arrival to last finish
+    rounds: int
+    stats: dict = field(default_factory=dict)
+
+    def latencies(self) -> np.ndarray:
+        return np.array([r.latency for r in self.results])
+
+
+def serve(ctx: Context, requests: list[Request], budget: int = 0,
+          clock=time.perf_counter) -> ServeReport:
+    """Run the request stream through one batch in real time."""
+    order = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
+    out: dict[int, Served] = {}
+    jobs: dict[int, int] = {}
+    rounds = 0
+    with Batch(ctx, budget) as b:
+        t0 = clock()
+        nxt = 0
+        busy = False
+        while len(out) < len(requests):
+            now = clock() - t0
+            while nxt < len(order) and requests[order[nxt]].arrival <= now:
+                i = order[nxt]
+                r = requests[i]
+                jobs[b.submit(r.graph, threshold=r.threshold, want_comm=r.want_comm)] = i
+                nxt += 1
+                busy = True
+            if not busy:
+                if nxt >= len(order):
+                    raise RuntimeError("serve: requests outstanding with nothing queued or running")
+                # nothing queued or running: wait for the next arrival
+                time.sleep(max(0.0, requests[order[nxt]].arrival - now))
+                continue
+            running, queued = b.step()
+            rounds += 1
+            t = clock() - t0
+            for j in b.poll():
+                i = jobs.pop(j)
+                res = b.result(j, want_comm=requests[i].want_comm)
+                out[i] = Served(i, requests[i].arrival, t, res.stats, res.comm)
+                b.forget(j)
+            busy = running > 0 or queued > 0
+        stats = b.stats()
+    results = [out[i] for i in range(len(requests))]
+    first = min(r.arrival for r in requests)
+    last = max(r.finish for r in results)
+    return ServeReport(results, last - first, rounds, stats)
+
+
+def fifo(arrivals, service) -> np.ndarray:
+    """Finish times of a single FIFO server: start = max(arrival, previous finish)."""
+    order = np.argsort(np.asarray(arrivals), kind="stable")
+    fin = np.empty(len(order))
+    t = -np.inf
+    for i in order:
+        t = max(t, arrivals[i]) + service[i]
+        fin[i] = t
+    return fin
+
+
+def sequential(ctx: Context, requests: list[Request]) -> ServeReport:
+    """The plain path: each request alone through vg_louvain_run, FIFO by arrival.
+
+    Service times are measured back to back; the FIFO queue (start = max(arrival,
+    previous finish)) then gives each request's finish time for the same arrivals.
+    """
+    import torch  # device timing on the library's stream
+
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    order = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
+    service = {}
+    levels = {}
+    comms = {}
+    for i in order:
+        r = requests[i]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = ctx.run(r.graph, threshold=r.threshold, want_comm=r.want_comm)
+        e1.record(stream)
+        e1.synchronize()
+        service[i] = e0.elapsed_time(e1) * 1e-3
+        levels[i] = res.stats
+        comms[i] = res.comm
+    arr = [r.arrival for r in requests]
+    svc = [service[i] for i in range(len(requests))]
+    fin = fifo(arr, svc)
+    res_list = [Served(i, arr[i], float(fin[i]), levels[i], comms[i]) for i in range(len(requests))]
+    return ServeReport(res_list, float(fin.max() - min(arr)), len(requests), {"service_s": svc})
+
+
+def percentile(x, q: float) -> float:
+    return float(np.percentile(np.asarray(x, dtype=np.float64), q))
