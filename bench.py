@@ -50,7 +50,8 @@ SERVE_REQUESTS = 96
 SERVE_E = (1e3, 5e7)              # CSR entries, log-uniform
 SERVE_SEED = 5151
 SERVE_LOAD = 8.0                  # offered load in units of the plain path's capacity
-SERVE_BUDGET = 48 << 30           # device-memory budget of the serving batch
+SERVE_BUDGET = 48 << 30           # device-memory budget of the serving batches
+SERVE_LANES = (1 << 18, 1 << 23)  # CSR-entry bounds of the size-class lanes
 REL_TOL = 1e-9
 
 
@@ -347,7 +348,7 @@ def run_serving(ctx, count: int) -> dict:
     fin = sv.fifo(arrivals, service)
     plain_lat = fin - arrivals
     ctx.reserve(SERVE_BUDGET)
-    served = sv.serve(ctx, reqs, budget=SERVE_BUDGET)
+    served = sv.serve(ctx, reqs, budget=SERVE_BUDGET, lanes=SERVE_LANES)
     lat = served.latencies()
     agree = sum(levels_agree(s.levels, p.levels) for s, p in zip(served.results, plain.results))
     for g in graphs:
@@ -356,10 +357,12 @@ def run_serving(ctx, count: int) -> dict:
         "workload": f"{count} requests, CSR entries log-uniform [{SERVE_E[0]:g}, {SERVE_E[1]:g}], "
                     f"RGG (distance weights) or Barabasi-Albert m=8 (U(0,1) weights), Poisson "
                     f"arrivals at {SERVE_LOAD:g}x the plain path's capacity, seed {SERVE_SEED}; "
-                    f"budget {SERVE_BUDGET >> 30} GiB; full multi-level Louvain",
+                    f"budget {SERVE_BUDGET >> 30} GiB, size-class lanes at "
+                    f"{'/'.join(str(x) for x in SERVE_LANES)} CSR entries; full multi-level Louvain",
         "requests": count, "csr_entries": int(sum(ne)), "rate_per_s": rate,
         "graphs_per_s": count / served.seconds, "p50_s": sv.percentile(lat, 50),
         "p99_s": sv.percentile(lat, 99), "rounds": served.rounds,
+        "lanes": served.stats["lanes"],
         "plain_graphs_per_s": count / float(fin.max() - arrivals.min()),
         "plain_p50_s": sv.percentile(plain_lat, 50), "plain_p99_s": sv.percentile(plain_lat, 99),
         "plain": "each request alone through vg_louvain_run, FIFO in arrival order (service "

@@ -14,7 +14,8 @@ def test_fifo_finish_times():
     assert list(fin) == [1.0, 2.0, 6.0]
 
 
-def test_served_results_equal_alone(ctx):
+@pytest.mark.parametrize("lanes", [(), (20000,)])
+def test_served_results_equal_alone(ctx, lanes):
     gs = []
     for k in range(10):
         if k % 2:
@@ -26,14 +27,15 @@ def test_served_results_equal_alone(ctx):
     alone = [ctx.run(g, want_comm=True) for g in gs]
     # arrivals spread over a few rounds, so later requests join a running batch
     reqs = [sv.Request(g, arrival=0.002 * k, want_comm=True) for k, g in enumerate(gs)]
-    rep = sv.serve(ctx, reqs, budget=1 << 30)
+    rep = sv.serve(ctx, reqs, budget=1 << 30, lanes=lanes)
     assert [r.index for r in rep.results] == list(range(len(gs)))
     for r, a in zip(rep.results, alone):
         assert r.latency >= 0.0
         assert [(x["nv"], x["ne"], x["iters"], x["modularity"]) for x in r.levels] == \
                [(x["nv"], x["ne"], x["iters"], x["modularity"]) for x in a.stats]
         assert np.array_equal(r.comm, a.comm)
-    assert rep.stats["completed"] == len(gs)
+    assert sum(l["requests"] for l in rep.stats["lanes"]) == len(gs)
+    assert len(rep.stats["lanes"]) == len(lanes) + 1
     seq = sv.sequential(ctx, reqs)
     for r, a in zip(seq.results, alone):
         assert [x["modularity"] for x in r.levels] == [x["modularity"] for x in a.stats]

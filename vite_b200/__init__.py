@@ -223,6 +223,7 @@ class Context:
         if st != VG_OK:
             raise VgError(st, f"vg_ctx_create(device={device}) failed")
         self.handle = h
+        self.device = device
 
     def close(self):
         if self.handle:

@@ -53,30 +53,28 @@ class ServeReport:
         return np.array([r.latency for r in self.results])
 
 
-def serve(ctx: Context, requests: list[Request], budget: int = 0,
-          clock=time.perf_counter) -> ServeReport:
-    """Run the request stream through one batch in real time."""
-    order = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
-    out: dict[int, Served] = {}
+def _lane_loop(ctx: Context, requests: list[Request], mine: list[int], budget: int, t0: float,
+               clock, out: dict, info: dict) -> None:
+    """One batch fed with the requests `mine` (sorted by arrival) in real time."""
     jobs: dict[int, int] = {}
     rounds = 0
     with Batch(ctx, budget) as b:
-        t0 = clock()
         nxt = 0
         busy = False
-        while len(out) < len(requests):
+        done = 0
+        while done < len(mine):
             now = clock() - t0
-            while nxt < len(order) and requests[order[nxt]].arrival <= now:
-                i = order[nxt]
+            while nxt < len(mine) and requests[mine[nxt]].arrival <= now:
+                i = mine[nxt]
                 r = requests[i]
                 jobs[b.submit(r.graph, threshold=r.threshold, want_comm=r.want_comm)] = i
                 nxt += 1
                 busy = True
             if not busy:
-                if nxt >= len(order):
+                if nxt >= len(mine):
                     raise RuntimeError("serve: requests outstanding with nothing queued or running")
                 # nothing queued or running: wait for the next arrival
-                time.sleep(max(0.0, requests[order[nxt]].arrival - now))
+                time.sleep(max(0.0, requests[mine[nxt]].arrival - now))
                 continue
             running, queued = b.step()
             rounds += 1
@@ -86,12 +84,67 @@ def serve(ctx: Context, requests: list[Request], budget: int = 0,
                 res = b.result(j, want_comm=requests[i].want_comm)
                 out[i] = Served(i, requests[i].arrival, t, res.stats, res.comm)
                 b.forget(j)
+                done += 1
             busy = running > 0 or queued > 0
-        stats = b.stats()
+        info["rounds"] = rounds
+        info["stats"] = b.stats()
+
+
+def serve(ctx: Context, requests: list[Request], budget: int = 0, lanes=(),
+          clock=time.perf_counter) -> ServeReport:
+    """Run the request stream in real time.
+
+    lanes: ascending CSR-entry bounds; with k bounds the requests are split into k+1
+    size classes, each served by its own batch on its own stream and host thread
+    (the last class keeps `ctx`), so the rounds of small graphs are not held to
+    the length of the largest graphs' phases. Each lane gets the whole budget
+    divided in proportion to its share of the requests' entries.
+    """
+    import threading
+
+    bounds = sorted(lanes)
+    sizes = [r.graph.ne for r in requests]
+    cls = [sum(1 for x in bounds if s > x) for s in sizes]
+    nl = len(bounds) + 1
+    order = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
+    mine = [[i for i in order if cls[i] == k] for k in range(nl)]
+    tot = max(sum(sizes), 1)
+    ctxs = [ctx if k == nl - 1 else Context(ctx.device) for k in range(nl)]
+    out: dict[int, Served] = {}
+    infos = [dict() for _ in range(nl)]
+    errors = []
+
+    def run(k, t0):
+        try:
+            if mine[k]:
+                share = sum(sizes[i] for i in mine[k]) / tot
+                # at least room for the lane's largest graph (the batch's own estimate:
+                # 40 bytes per CSR entry, 200 per vertex, 1 MiB)
+                big = max(40 * requests[i].graph.ne + 200 * requests[i].graph.nv + (1 << 20)
+                          for i in mine[k])
+                bud = 0 if budget == 0 else max(int(budget * share), big)
+                _lane_loop(ctxs[k], requests, mine[k], bud, t0, clock, out, infos[k])
+        except BaseException as e:  # re-raised in the caller
+            errors.append(e)
+
+    try:
+        t0 = clock()
+        threads = [threading.Thread(target=run, args=(k, t0)) for k in range(nl)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+    finally:
+        for k in range(nl - 1):
+            ctxs[k].close()
+    if errors:
+        raise errors[0]
     results = [out[i] for i in range(len(requests))]
     first = min(r.arrival for r in requests)
     last = max(r.finish for r in results)
-    return ServeReport(results, last - first, rounds, stats)
+    stats = {"lanes": [{"requests": len(mine[k]), "rounds": infos[k].get("rounds", 0)}
+                       for k in range(nl)]}
+    return ServeReport(results, last - first, sum(i.get("rounds", 0) for i in infos), stats)
 
 
 def fifo(arrivals, service) -> np.ndarray:
