@@ -14,8 +14,9 @@
 // The locality order is computed on the device from the graph alone: a
 // multi-source breadth-first search from hashed seeds (about one seed per 1024
 // vertices) labels each vertex with its nearest seed, and vertices are ordered by
-// (seed, BFS distance, id), so a cluster occupies a contiguous range of positions
-// and most neighbours of a vertex lie in the same few cache lines.
+// (seed, degree bucket, BFS distance, id), so a cluster occupies a contiguous range
+// of positions, most neighbours of a vertex lie in the same few cache lines, and
+// 32 consecutive vertices mostly share a degree bucket.
 #include "vg_internal.cuh"
 
 #include <algorithm>
@@ -85,14 +86,23 @@ __global__ void k_bfs_step(const int64_t *__restrict__ rowptr, const int32_t *__
     if ((threadIdx.x & 31) == 0 && mine) atomicAdd(claimed, mine);
 }
 
-__global__ void k_order_keys(int64_t nv, const int32_t *__restrict__ label,
-                             const uint8_t *__restrict__ dist, uint64_t *__restrict__ keys,
-                             uint32_t *__restrict__ vals) {
+// degree bucket of the order key: the sweep's short-row kernel runs each warp of
+// 32 consecutive vertices with loops as long as its largest row, so vertices of
+// similar degree are kept together inside a cluster
+__device__ __forceinline__ uint32_t degree_bucket(int64_t d) {
+    return d <= 8 ? 0u : d <= 12 ? 1u : d <= 16 ? 2u : d <= 32 ? 3u : 4u;
+}
+
+__global__ void k_order_keys(int64_t nv, const int64_t *__restrict__ rowptr,
+                             const int32_t *__restrict__ label, const uint8_t *__restrict__ dist,
+                             uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
          v += (int64_t)gridDim.x * blockDim.x) {
         const int32_t l = label[v];
-        // unreached vertices (components without a seed) keep their own place
-        keys[v] = l < 0 ? ((uint64_t)v << 8) : (((uint64_t)l << 8) | dist[v]);
+        const uint64_t b = degree_bucket(rowptr[v + 1] - rowptr[v]);
+        // (cluster, degree bucket, BFS distance); unreached vertices (components
+        // without a seed) keep their own place
+        keys[v] = l < 0 ? ((uint64_t)v << 12) : (((uint64_t)l << 12) | (b << 8) | dist[v]);
         vals[v] = (uint32_t)v;
     }
 }
@@ -213,11 +223,12 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
     }
     DevBuf<uint64_t> keys(ctx, nv);
     DevBuf<uint32_t> vals(ctx, nv);
-    { LaunchTimer lt(ctx); k_order_keys<<<grid, 256, 0, ctx->stream>>>(nv, label.p, dist.p, keys.p, vals.p); }
+    { LaunchTimer lt(ctx);
+      k_order_keys<<<grid, 256, 0, ctx->stream>>>(nv, g->rowptr, label.p, dist.p, keys.p, vals.p); }
     VG_CHECK_LAUNCH();
     int bits = 1;
     while (bits < 40 && ((int64_t)1 << bits) < nv) bits++;
-    vg_radix_sort_pairs(ctx, keys.p, vals.p, nv, bits + 8);
+    vg_radix_sort_pairs(ctx, keys.p, vals.p, nv, bits + 12);
     VG_CUDA(cudaMemcpyAsync(order.p, vals.p, sizeof(int32_t) * nv, cudaMemcpyDeviceToDevice,
                             ctx->stream));
 }

@@ -230,19 +230,101 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? 3 : 3)) k_sweep_thread(
     }
 }
 
+// one vertex of a tile (degree d <= T): counters fold in place in the staged
+// weights of its row, in CSR order, at the slot of each community's first occurrence
+template <int T>
+__device__ __forceinline__ void tile_vertex(const SweepArgs &a, int32_t v, int d, double cst,
+                                            const int32_t *ts, double *ws) {
+    if (a.active && !a.active[v]) {
+        a.cw[v] = a.frozen[v];
+        return;
+    }
+    const int32_t cc = __ldg(a.curr + v);
+    const double vd = a.vdeg[v];
+    const double ccDeg = __ldg(a.cdeg + cc);
+    int32_t c[T];
+    double selfLoop = 0.0;
+#pragma unroll
+    for (int j = 0; j < T; j++) {
+        c[j] = -1;
+        if (j < d) c[j] = __ldg(a.curr + ts[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < T; j++)
+        if (j < d && ts[j] == v) selfLoop = __dadd_rn(selfLoop, ws[j]);
+    uint32_t first = 0;
+#pragma unroll
+    for (int j = 0; j < T; j++) {
+        if (j < d) {
+            int fj = j;
+#pragma unroll
+            for (int k = j - 1; k >= 0; k--)
+                if (c[k] == c[j]) fj = k;
+            if (fj == j) first |= 1u << j;
+            else ws[fj] = __dadd_rn(ws[fj], ws[j]);
+        }
+    }
+    double counter0 = 0.0;
+#pragma unroll
+    for (int j = 0; j < T; j++)
+        if (((first >> j) & 1u) && c[j] == cc) counter0 = ws[j];
+    const double eix = __dsub_rn(counter0, selfLoop);
+    const double ax = __dsub_rn(ccDeg, vd);
+    double bg = 0.0;
+    int32_t bc = INT_MAX;
+    bool ok = false;
+#pragma unroll
+    for (int b = 0; b < T; b += 8) {
+        double ay[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int j = b + q;
+            ay[q] = 0.0;
+            if (j < T && ((first >> j) & 1u) && c[j] != cc) ay[q] = __ldg(a.cdeg + c[j]);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int j = b + q;
+            if (j < T && ((first >> j) & 1u) && c[j] != cc) {
+                const double g = gain_of(ws[j], eix, vd, ay[q], ax, cst);
+                if (g > 0.0 && better(true, g, c[j], ok, bg, bc, a.ref)) {
+                    bg = g;
+                    bc = c[j];
+                    ok = true;
+                }
+            }
+        }
+    }
+    int32_t ccSize = 0, bs = 0;
+    if (ok && vg_rid(a.ref, bc) > vg_rid(a.ref, cc)) {
+        ccSize = __ldg(a.csize + cc);
+        bs = __ldg(a.csize + bc);
+    }
+    commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, bc, bs);
+}
+
 // ---------------------------------------------------------------------------------
-// class 0 in vertex order: a warp takes 32 consecutive vertices, whose rows form
-// one contiguous edge range, and stages that range into shared memory with
-// coalesced 128-bit loads; each lane then works on its own vertex from shared
+// class 0 in vertex order: a warp takes a tile of 32 consecutive vertices, whose
+// rows form one contiguous edge range, and stages that range into shared memory
+// with coalesced 128-bit loads; each lane then works on its own vertex from shared
 // memory. Counters fold in place, in the staged weights of the lane's row, in
 // CSR order (slot of the community's first occurrence). A range longer than the
 // staging buffer falls back to per-lane copies of the (short) rows.
 
 constexpr int TILE_CAP = 504;          // staged edges per warp (48 KB of shared memory per CTA)
-constexpr int TILE_WARPS = 8;
+#ifndef VG_TILE_WARPS
+#define VG_TILE_WARPS 8
+#endif
+#ifndef VG_TILE_MINB
+#define VG_TILE_MINB 4 // resident CTAs per SM the register budget is sized for
+#endif
+#ifndef VG_TILE_GRID
+#define VG_TILE_GRID 8 // CTAs per SM in the grid
+#endif
+constexpr int TILE_WARPS = VG_TILE_WARPS;
 
 template <int T>
-__global__ void __launch_bounds__(TILE_WARPS * 32, 4) k_sweep_tile(SweepArgs a, int64_t nv) {
+__global__ void __launch_bounds__(TILE_WARPS * 32, VG_TILE_MINB) k_sweep_tile(SweepArgs a, int64_t nv) {
     static_assert(32 * T <= TILE_CAP + 8, "the per-lane fallback layout must fit the buffer");
     __shared__ int32_t st_all[TILE_WARPS][TILE_CAP + 8];
     __shared__ double sw_all[TILE_WARPS][TILE_CAP + 8];
@@ -309,76 +391,7 @@ __global__ void __launch_bounds__(TILE_WARPS * 32, 4) k_sweep_tile(SweepArgs a, 
             off_w = lane * T;
         }
         __syncwarp();
-        if (live && d <= T) {
-            if (a.active && !a.active[v]) {
-                a.cw[v] = a.frozen[v];
-            } else {
-                const int32_t *ts = st + off_t;
-                double *ws = sw + off_w;
-                const int32_t cc = __ldg(a.curr + v);
-                const double vd = a.vdeg[v];
-                const double ccDeg = __ldg(a.cdeg + cc);
-                int32_t c[T];
-                double selfLoop = 0.0;
-#pragma unroll
-                for (int j = 0; j < T; j++) {
-                    c[j] = -1;
-                    if (j < d) c[j] = __ldg(a.curr + ts[j]);
-                }
-#pragma unroll
-                for (int j = 0; j < T; j++)
-                    if (j < d && ts[j] == v) selfLoop = __dadd_rn(selfLoop, ws[j]);
-                uint32_t first = 0;
-#pragma unroll
-                for (int j = 0; j < T; j++) {
-                    if (j < d) {
-                        int fj = j;
-#pragma unroll
-                        for (int k = j - 1; k >= 0; k--)
-                            if (c[k] == c[j]) fj = k;
-                        if (fj == j) first |= 1u << j;
-                        else ws[fj] = __dadd_rn(ws[fj], ws[j]);
-                    }
-                }
-                double counter0 = 0.0;
-#pragma unroll
-                for (int j = 0; j < T; j++)
-                    if (((first >> j) & 1u) && c[j] == cc) counter0 = ws[j];
-                const double eix = __dsub_rn(counter0, selfLoop);
-                const double ax = __dsub_rn(ccDeg, vd);
-                double bg = 0.0;
-                int32_t bc = INT_MAX;
-                bool ok = false;
-#pragma unroll
-                for (int b = 0; b < T; b += 8) {
-                    double ay[8];
-#pragma unroll
-                    for (int q = 0; q < 8; q++) {
-                        const int j = b + q;
-                        ay[q] = 0.0;
-                        if (((first >> j) & 1u) && c[j] != cc) ay[q] = __ldg(a.cdeg + c[j]);
-                    }
-#pragma unroll
-                    for (int q = 0; q < 8; q++) {
-                        const int j = b + q;
-                        if (((first >> j) & 1u) && c[j] != cc) {
-                            const double g = gain_of(ws[j], eix, vd, ay[q], ax, cst);
-                            if (g > 0.0 && better(true, g, c[j], ok, bg, bc, a.ref)) {
-                                bg = g;
-                                bc = c[j];
-                                ok = true;
-                            }
-                        }
-                    }
-                }
-                int32_t ccSize = 0, bs = 0;
-                if (ok && vg_rid(a.ref, bc) > vg_rid(a.ref, cc)) {
-                    ccSize = __ldg(a.csize + cc);
-                    bs = __ldg(a.csize + bc);
-                }
-                commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, bc, bs);
-            }
-        }
+        if (live && d <= T) tile_vertex<T>(a, v, d, cst, st + off_t, sw + off_w);
         __syncwarp();
     }
 }
@@ -1215,7 +1228,7 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
         if (cls == 0 && natural) {
             if (nv == 0) continue;
             LaunchTimer lt(ctx);
-            k_sweep_tile<TMAX><<<vg_grid(ctx, nv, TILE_WARPS * 32, 8), TILE_WARPS * 32, 0,
+            k_sweep_tile<TMAX><<<vg_grid(ctx, nv, TILE_WARPS * 32, VG_TILE_GRID), TILE_WARPS * 32, 0,
                                  ctx->stream>>>(a, nv);
             VG_CHECK_LAUNCH();
             continue;
