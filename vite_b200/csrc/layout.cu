@@ -39,12 +39,14 @@ __global__ void k_bfs_init(int64_t nv, uint64_t seed, int32_t *__restrict__ labe
 // one level: vertices at distance step-1 claim their unlabeled neighbours. A warp
 // takes 32 consecutive vertices; a frontier row of at most 64 entries is scanned
 // by its own lane, a longer one by the whole warp.
+// unvisited vertices are found through the byte array of distances (255 =
+// unvisited), which stays in L2; the label's compare-and-swap settles races
 __device__ __forceinline__ unsigned long long bfs_claim(const int32_t *__restrict__ tail, int64_t e,
                                                         int32_t lu, int step,
                                                         int32_t *__restrict__ label,
                                                         uint8_t *__restrict__ dist) {
     const int32_t w = tail[e];
-    if (label[w] == -1 && atomicCAS(&label[w], -1, lu) == -1) {
+    if (dist[w] == 255 && atomicCAS(&label[w], -1, lu) == -1) {
         dist[w] = (uint8_t)step;
         return 1;
     }
@@ -122,18 +124,19 @@ __global__ void k_gather_deg(const int64_t *__restrict__ rowptr, const int32_t *
     }
 }
 
-// new row k = old row from[k], tails renamed through `rename`, entry order kept
+// new row k = old row from[k], tails renamed through `rename`, entry order kept;
+// eight lanes per row (rows are short)
 __global__ void k_move_rows(const int64_t *__restrict__ rp, const int32_t *__restrict__ tail,
                             const double *__restrict__ w, int64_t n, const int32_t *__restrict__ from,
                             const int32_t *__restrict__ rename, const int64_t *__restrict__ rp2,
                             int32_t *__restrict__ tail2, double *__restrict__ w2) {
-    const int lane = threadIdx.x & 31;
-    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t k = wg; k < n; k += nw) {
+    const int sub = threadIdx.x & 7;
+    const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
+    for (int64_t k = grp; k < n; k += ng) {
         const int32_t r = from[k];
         const int64_t s = rp[r], len = rp[r + 1] - s, o = rp2[k];
-        for (int64_t j = lane; j < len; j += 32) {
+        for (int64_t j = sub; j < len; j += 8) {
             tail2[o + j] = rename[tail[s + j]];
             w2[o + j] = w[s + j];
         }
@@ -193,7 +196,7 @@ static vg_graph *move_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *from,
     DevBuf<double> w(ctx, ne);
     if (nv) {
         LaunchTimer lt(ctx);
-        k_move_rows<<<vg_grid(ctx, nv * 32, 256), 256, 0, ctx->stream>>>(
+        k_move_rows<<<vg_grid(ctx, nv * 8, 256), 256, 0, ctx->stream>>>(
             g->rowptr, g->tail, g->weight, nv, from, rename, rp.p, tail.p, w.p);
     }
     VG_CHECK_LAUNCH();
