@@ -49,20 +49,75 @@ __global__ void k_row_starts(const uint64_t *__restrict__ keys, const int64_t *_
         if (k == 0 || keys[k] != keys[k - 1]) rstart[keys[k]] = off[k];
 }
 
-// one warp per vertex (in grouped order): its row goes to the segment, neighbours
-// renamed to their ordering keys
+// Rows of at most LONG_ROW entries are copied by eight lanes each; the longer ones
+// (hubs, giant communities) are cut into chunks of COPY_CHUNK entries, one block per
+// chunk, so one row never serialises a warp.
+constexpr int64_t LONG_ROW = 4096;
+constexpr int64_t COPY_CHUNK = 4096;
+
+// vertices in grouped order: each one's row goes to its segment, neighbours renamed
+// to their ordering keys
 __global__ void k_group_copy(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
                              const double *__restrict__ w, const int32_t *__restrict__ pos,
                              const uint32_t *__restrict__ order, const int64_t *__restrict__ off,
                              int64_t nv, const int32_t *__restrict__ new_key,
                              int32_t *__restrict__ gk, double *__restrict__ gw) {
-    const int lane = threadIdx.x & 31;
-    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t k = wg; k < nv; k += nw) {
+    const int sub = threadIdx.x & 7;
+    const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
+    for (int64_t k = grp; k < nv; k += ng) {
+        const int64_t o = off[k], len = off[k + 1] - o;
+        if (len > LONG_ROW) continue;
         const int32_t p = pos_of(pos, order[k]);
-        const int64_t e0 = rowptr[p], len = rowptr[p + 1] - e0, o = off[k];
-        for (int64_t j = lane; j < len; j += 32) {
+        const int64_t e0 = rowptr[p];
+        for (int64_t j = sub; j < len; j += 8) {
+            gk[o + j] = new_key[tail[e0 + j]];
+            gw[o + j] = w[e0 + j];
+        }
+    }
+}
+
+// rows [offs[r], offs[r+1]) longer than LONG_ROW: their list and chunk counts
+__global__ void k_long_flags(const int64_t *__restrict__ offs, int64_t n, int32_t *__restrict__ flag) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+         r += (int64_t)gridDim.x * blockDim.x)
+        flag[r] = offs[r + 1] - offs[r] > LONG_ROW ? 1 : 0;
+}
+
+__global__ void k_long_place(const int32_t *__restrict__ flag, const int64_t *__restrict__ idx,
+                             int64_t n, const int64_t *__restrict__ offs,
+                             int32_t *__restrict__ list, int64_t *__restrict__ nch) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+         r += (int64_t)gridDim.x * blockDim.x)
+        if (flag[r]) {
+            list[idx[r]] = (int32_t)r;
+            nch[idx[r]] = (offs[r + 1] - offs[r] + COPY_CHUNK - 1) / COPY_CHUNK;
+        }
+}
+
+__device__ __forceinline__ int64_t chunk_owner(const int64_t *__restrict__ cb, int64_t n, int64_t c) {
+    int64_t lo = 0, hi = n; // largest q with cb[q] <= c
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (cb[mid] <= c) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_group_copy_long(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
+                                  const double *__restrict__ w, const int32_t *__restrict__ pos,
+                                  const uint32_t *__restrict__ order, const int64_t *__restrict__ off,
+                                  const int32_t *__restrict__ list, const int64_t *__restrict__ cb,
+                                  int64_t nl, int64_t nchunks, const int32_t *__restrict__ new_key,
+                                  int32_t *__restrict__ gk, double *__restrict__ gw) {
+    for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const int64_t q = chunk_owner(cb, nl, c);
+        const int64_t k = list[q];
+        const int64_t o = off[k], len = off[k + 1] - o;
+        const int64_t e0 = rowptr[pos_of(pos, order[k])];
+        const int64_t j0 = (c - cb[q]) * COPY_CHUNK, j1 = min(j0 + COPY_CHUNK, len);
+        for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
             gk[o + j] = new_key[tail[e0 + j]];
             gw[o + j] = w[e0 + j];
         }
@@ -335,17 +390,61 @@ __global__ void k_compact_rows(int64_t nc, const int64_t *__restrict__ rstart,
                                const int64_t *__restrict__ rowptr, const int32_t *__restrict__ uk,
                                const double *__restrict__ uw, const int32_t *__restrict__ key_to_pos,
                                int32_t *__restrict__ tail, double *__restrict__ w) {
-    const int lane = threadIdx.x & 31;
-    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t row = wg; row < nc; row += nw) {
+    const int sub = threadIdx.x & 7;
+    const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
+    for (int64_t row = grp; row < nc; row += ng) {
         const int64_t s = rstart[row], o = rowptr[row], len = rowptr[row + 1] - o;
-        for (int64_t j = lane; j < len; j += 32) {
+        if (len > LONG_ROW) continue;
+        for (int64_t j = sub; j < len; j += 8) {
             const int32_t k = uk[s + j];
             tail[o + j] = key_to_pos ? key_to_pos[k] : k;
             w[o + j] = uw[s + j];
         }
     }
+}
+
+__global__ void k_compact_long(const int64_t *__restrict__ rstart, const int64_t *__restrict__ rowptr,
+                               const int32_t *__restrict__ list, const int64_t *__restrict__ cb,
+                               int64_t nl, int64_t nchunks, const int32_t *__restrict__ uk,
+                               const double *__restrict__ uw, const int32_t *__restrict__ key_to_pos,
+                               int32_t *__restrict__ tail, double *__restrict__ w) {
+    for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const int64_t q = chunk_owner(cb, nl, c);
+        const int64_t row = list[q];
+        const int64_t s = rstart[row], o = rowptr[row], len = rowptr[row + 1] - o;
+        const int64_t j0 = (c - cb[q]) * COPY_CHUNK, j1 = min(j0 + COPY_CHUNK, len);
+        for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            const int32_t k = uk[s + j];
+            tail[o + j] = key_to_pos ? key_to_pos[k] : k;
+            w[o + j] = uw[s + j];
+        }
+    }
+}
+
+// the rows of offs (n + 1 offsets) longer than LONG_ROW, with their chunk prefix
+struct LongRows {
+    DevBuf<int32_t> list;
+    DevBuf<int64_t> cb;
+    int64_t n = 0, nch = 0;
+};
+
+void long_rows(vg_ctx *ctx, const int64_t *offs, int64_t n, LongRows &L) {
+    if (n == 0) return;
+    DevBuf<int32_t> flag(ctx, n);
+    DevBuf<int64_t> idx(ctx, n);
+    { LaunchTimer lt(ctx);
+      k_long_flags<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(offs, n, flag.p); }
+    VG_CHECK_LAUNCH();
+    L.n = vg_exclusive_scan_i32_to_i64(ctx, flag.p, idx.p, n);
+    if (L.n == 0) return;
+    L.list.alloc(ctx, L.n);
+    L.cb.alloc(ctx, L.n + 1);
+    { LaunchTimer lt(ctx);
+      k_long_place<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(flag.p, idx.p, n, offs, L.list.p,
+                                                                  L.cb.p); }
+    VG_CHECK_LAUNCH();
+    L.nch = vg_exclusive_scan_i64(ctx, L.cb.p, L.n);
 }
 
 } // namespace
@@ -397,10 +496,21 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     DevBuf<double> gw(ctx, ne);
     if (ne) {
         LaunchTimer lt(ctx);
-        k_group_copy<<<vg_grid(ctx, nv * 32, 256), 256, 0, ctx->stream>>>(
+        k_group_copy<<<vg_grid(ctx, nv * 8, 256), 256, 0, ctx->stream>>>(
             g->rowptr, g->tail, g->weight, pos, vorder.p, off.p, nv, new_key, gk.p, gw.p);
     }
     VG_CHECK_LAUNCH();
+    {
+        LongRows L;
+        long_rows(ctx, off.p, nv, L);
+        if (L.nch) {
+            LaunchTimer lt(ctx);
+            k_group_copy_long<<<(int)std::min<int64_t>(L.nch, 16LL * ctx->sm_count), 256, 0,
+                                ctx->stream>>>(g->rowptr, g->tail, g->weight, pos, vorder.p, off.p,
+                                               L.list.p, L.cb.p, L.n, L.nch, new_key, gk.p, gw.p);
+        }
+        VG_CHECK_LAUNCH();
+    }
     vorder.release();
     off.release();
     // 4. sort + fold per segment
@@ -480,10 +590,21 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     DevBuf<double> w(ctx, m);
     if (nc) {
         LaunchTimer lt(ctx);
-        k_compact_rows<<<vg_grid(ctx, nc * 32, 256), 256, 0, ctx->stream>>>(
+        k_compact_rows<<<vg_grid(ctx, nc * 8, 256), 256, 0, ctx->stream>>>(
             nc, rstart.p, ucount.p, uk.p, uw.p, key_to_pos, tail.p, w.p);
     }
     VG_CHECK_LAUNCH();
+    {
+        LongRows L;
+        long_rows(ctx, ucount.p, nc, L);
+        if (L.nch) {
+            LaunchTimer lt(ctx);
+            k_compact_long<<<(int)std::min<int64_t>(L.nch, 16LL * ctx->sm_count), 256, 0,
+                             ctx->stream>>>(rstart.p, ucount.p, L.list.p, L.cb.p, L.n, L.nch, uk.p,
+                                            uw.p, key_to_pos, tail.p, w.p);
+        }
+        VG_CHECK_LAUNCH();
+    }
     vg_sync(ctx);
     return vg_graph_wrap(ctx, nc, m, ucount.detach(), tail.detach(), w.detach());
 }

@@ -173,6 +173,40 @@ extern "C" vg_status vg_ctx_profile(vg_ctx *ctx, int32_t enable, double *kernel_
 // ---------------------------------------------------------------------------------
 // graphs
 
+namespace {
+__global__ void k_integral(const double *__restrict__ w, int64_t ne, int *__restrict__ bad) {
+    int mine = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ne;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = w[i];
+        if (!(fabs(x) <= 1048576.0) || x != floor(x)) mine = 1;
+    }
+    if (__any_sync(0xffffffffu, mine) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
+}
+} // namespace
+
+bool vg_weights_integral(vg_ctx *ctx, vg_graph *g) {
+    if (g->integral >= 0) return g->integral == 1;
+    int r = 1;
+    if (g->ne >= ((int64_t)1 << 31)) {
+        r = 0;
+    } else if (g->ne > 0) {
+        DevBuf<int> bad(ctx, 1);
+        VG_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
+        {
+            LaunchTimer lt(ctx);
+            k_integral<<<vg_grid(ctx, g->ne, 256), 256, 0, ctx->stream>>>(g->weight, g->ne, bad.p);
+        }
+        VG_CHECK_LAUNCH();
+        int *h = (int *)vg_pinned(ctx, sizeof(int));
+        VG_CUDA(cudaMemcpyAsync(h, bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        vg_sync(ctx);
+        r = *h ? 0 : 1;
+    }
+    g->integral = (int8_t)r;
+    return r == 1;
+}
+
 vg_graph *vg_graph_wrap(vg_ctx *ctx, int64_t nv, int64_t ne, int64_t *rowptr, int32_t *tail,
                         double *weight) {
     (void)ctx;

@@ -250,6 +250,7 @@ vg_graph *vg_apply_layout(vg_ctx *ctx, const vg_graph *g, const int32_t *order) 
     vg_graph *h = move_rows(ctx, g, order, pos.p);
     h->ref = ref.detach();
     h->pos = pos.detach();
+    h->integral = g->integral;
     return h;
 }
 

@@ -726,12 +726,13 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
 
 // distSumVertexDegree (louvain.cpp:2161-2186): each row summed in CSR order. A
 // warp takes 32 consecutive rows; a row of at most DEG_LONG entries is summed by
-// its own lane, a longer one by the whole warp: coalesced loads of 32 entries,
-// added one after the other (every lane forms the same left fold).
+// its own lane. A longer row: with integral weights every order gives the same
+// exact sum, so the warp adds it as a tree; otherwise one lane forms the left
+// fold, its loads issued eight at a time ahead of the ordered additions.
 constexpr int DEG_LONG = 64;
 
 __global__ void k_degree(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
-                         int64_t nv, double *__restrict__ vdeg) {
+                         int64_t nv, double *__restrict__ vdeg, int integral) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -756,10 +757,23 @@ __global__ void k_degree(const int64_t *__restrict__ rowptr, const double *__res
             lm &= lm - 1;
             const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
             double sum = 0.0;
-            for (int64_t off = E0; off < E1; off += 32) {
-                const double x = off + lane < E1 ? w[off + lane] : 0.0;
-                const int n = (int)min((int64_t)32, E1 - off);
-                for (int q = 0; q < n; q++) sum = __dadd_rn(sum, __shfl_sync(full, x, q));
+            if (integral) {
+                for (int64_t k = E0 + lane; k < E1; k += 32) sum = __dadd_rn(sum, w[k]);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) sum = __dadd_rn(sum, __shfl_xor_sync(full, sum, o));
+            } else {
+                if (lane == 0) {
+                    int64_t k = E0;
+                    for (; k + 8 <= E1; k += 8) {
+                        double x[8];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) x[t] = w[k + t];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) sum = __dadd_rn(sum, x[t]);
+                    }
+                    for (; k < E1; k++) sum = __dadd_rn(sum, w[k]);
+                }
+                sum = __shfl_sync(full, sum, 0);
             }
             if (lane == src) vdeg[v] = sum;
         }
@@ -1302,9 +1316,10 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
     }
     const int grid = vg_grid(ctx, nv, 256);
     if (nv) {
+        const int integ = (int)vg_weights_integral(ctx, g);
         {
             LaunchTimer lt(ctx);
-            k_degree<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->weight, nv, vdeg.p);
+            k_degree<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->weight, nv, vdeg.p, integ);
         }
         VG_CHECK_LAUNCH();
     }
@@ -1485,9 +1500,10 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
     DevBuf<CommInfo> cupd(ctx, nv);
     DevBuf<int32_t> B0(ctx, nv), B1(ctx, nv), B2(ctx, nv);
     const int grid = vg_grid(ctx, nv, 256);
+    const int integ = (int)vg_weights_integral(ctx, U);
     {
         LaunchTimer lt(ctx);
-        k_degree<<<grid, 256, 0, ctx->stream>>>(U->rowptr, U->weight, nv, vdeg.p);
+        k_degree<<<grid, 256, 0, ctx->stream>>>(U->rowptr, U->weight, nv, vdeg.p, integ);
     }
     VG_CHECK_LAUNCH();
     // per-graph 2m in each graph's own fixed order, 1/(2m) on the host as in the plain path
@@ -1672,9 +1688,10 @@ extern "C" vg_status vg_vertex_degree(vg_ctx *ctx, vg_graph *g, double *vdeg_out
         VG_CUDA(cudaSetDevice(ctx->device));
         DevBuf<double> vdeg(ctx, g->nv);
         if (g->nv) {
+            const int integ = (int)vg_weights_integral(ctx, g);
             LaunchTimer lt(ctx);
             k_degree<<<vg_grid(ctx, g->nv, 256), 256, 0, ctx->stream>>>(g->rowptr, g->weight, g->nv,
-                                                                         vdeg.p);
+                                                                         vdeg.p, integ);
         }
         VG_CHECK_LAUNCH();
         const double tm = g->nv ? twice_m_one(ctx, vdeg.p, g->nv) : 0.0;

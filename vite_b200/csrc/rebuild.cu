@@ -142,7 +142,9 @@ vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm) {
         first.release();
         flag.release();
         rank.release();
-        return vg_aggregate_rows(ctx, g, nullptr, newof.p, newof.p, nc, nullptr);
+        vg_graph *h = vg_aggregate_rows(ctx, g, nullptr, newof.p, newof.p, nc, nullptr);
+        h->integral = g->integral == 1 ? 1 : -1; // sums of the same integers
+        return h;
     }
     DevBuf<int32_t> first_ref(ctx, nv), first_pos(ctx, nv), flag_ref(ctx, nv), flag_pos(ctx, nv);
     DevBuf<int64_t> rank_ref(ctx, nv), rank_pos(ctx, nv);
@@ -184,6 +186,7 @@ vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm) {
     }
     h->ref = r2.detach();
     h->pos = p2.detach();
+    h->integral = g->integral == 1 ? 1 : -1; // sums of the same integers
     return h;
 }
 
@@ -683,6 +686,7 @@ extern "C" vg_status vg_graph_reweight(vg_ctx *ctx, vg_graph *g, int32_t mode, u
                                                                                g->weight, g->nv, mode, seed);
         }
         VG_CHECK_LAUNCH();
+        g->integral = -1; // the weights changed
         vg_sync(ctx);
     });
 }

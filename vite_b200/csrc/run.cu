@@ -70,6 +70,8 @@ extern "C" vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g0, const vg_ru
         VG_REQUIRE(!((rp->et_type == 2 || rp->et_type == 4) &&
                      (rp->et_delta > 1.0 || rp->et_delta < 0.0)),
                    "early-term-alpha must be between 0 and 1");
+        // whether sums of g0's weights are exact in any order: computed once, cached on g0
+        vg_weights_integral(ctx, const_cast<vg_graph *>(g0));
         // level 0 runs on a shallow view of g0 so that its attached state stays untouched
         vg_graph view = *g0;
         view.colors = nullptr;

@@ -127,7 +127,14 @@ struct vg_graph {
     // inverse. Both null when positions are the reference ids.
     int32_t *ref = nullptr;
     int32_t *pos = nullptr;
+    // 1: every weight is an integer of magnitude at most 2^20 (and ne < 2^31), so
+    // every sum of weights is an exact integer below 2^51 whatever its order;
+    // 0: not so; -1: not yet known (vg_weights_integral computes it)
+    int8_t integral = -1;
 };
+
+// whether g's weights are integral in the sense above (computed once per graph)
+bool vg_weights_integral(vg_ctx *ctx, vg_graph *g);
 
 // reference id of the vertex (or community) at position p
 __device__ __forceinline__ int32_t vg_rid(const int32_t *__restrict__ ref, int32_t p) {
