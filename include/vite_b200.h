@@ -66,8 +66,10 @@ typedef struct vg_run_params {
     int32_t one_phase;         /* -p */
     int32_t layout;            /* HBM layout of the level-0 graph: 0 as given, 1 locality order
                                   computed on the device (vg_graph_reorder mode 1), 2 locality
-                                  order when the graph has at least 2^18 vertices. Results are
-                                  the same in every layout. */
+                                  order when the graph has at least 2^18 vertices and local
+                                  structure (a sampled clustering coefficient of at least 0.1:
+                                  geometric graphs yes, preferential-attachment and uniform
+                                  random graphs no). Results are the same in every layout. */
 } vg_run_params;
 
 /* What graphClustering prints per level (main.cpp:465-474), measured on the device. */

@@ -248,8 +248,7 @@ void pack(vg_batch *b, const std::vector<int64_t> &keep, const std::vector<int64
         BJob &j = *b->jobs.at(id);
         const vg_graph *g = j.src;
         vg_graph *lg = nullptr;
-        const int lay = j.rp.layout;
-        if (!g->ref && (lay == 1 || (lay == 2 && g->nv >= (1 << 18)))) {
+        if (vg_auto_layout(ctx, g, j.rp.layout)) {
             // the locality layout the plain path gives a graph of this size
             DevBuf<int32_t> ord;
             vg_bfs_order(ctx, g, ord);

@@ -176,7 +176,68 @@ __global__ void k_ref_to_pos(const int32_t *__restrict__ in, int64_t n,
     }
 }
 
+// Local structure test: for a hashed sample of vertices, pairs of neighbours (u, w)
+// are checked for an edge u-w (the clustering coefficient). Geometric graphs have
+// a high one (about 0.59 for a 2-D random geometric graph), preferential-attachment
+// and uniform random graphs a vanishing one; only the former gain from the
+// locality layout. One warp per sampled vertex; u's row is scanned up to SCAN_CAP.
+constexpr int CC_SAMPLE = 4096;
+constexpr int CC_PAIRS = 8;
+constexpr int CC_SCAN_CAP = 256;
+
+__global__ void k_cc_sample(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
+                            int64_t nv, uint64_t seed, unsigned long long *__restrict__ counts) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long hits = 0, pairs = 0;
+    for (int64_t s = wg; s < CC_SAMPLE; s += nw) {
+        const int64_t v = (int64_t)vg_uint_below(vg_mix(seed, 43, (uint64_t)s), (uint64_t)nv);
+        const int64_t e0 = rowptr[v], d = rowptr[v + 1] - e0;
+        if (d < 2) continue;
+        for (int p = 0; p < CC_PAIRS; p++) {
+            const uint64_t r = vg_mix(seed, 44, (uint64_t)(s * CC_PAIRS + p));
+            const int64_t i = (int64_t)vg_uint_below(r, (uint64_t)d);
+            int64_t j = (int64_t)vg_uint_below(r * 0x9E3779B97F4A7C15ULL + 1, (uint64_t)(d - 1));
+            if (j >= i) j++;
+            const int32_t u = tail[e0 + i], w = tail[e0 + j];
+            if (u == w || u == v || w == v) continue;
+            const int64_t f0 = rowptr[u], f1 = min(rowptr[u + 1], f0 + CC_SCAN_CAP);
+            bool found = false;
+            for (int64_t k = f0 + lane; k < f1; k += 32) found |= tail[k] == w;
+            found = __any_sync(0xffffffffu, found);
+            if (lane == 0) {
+                pairs++;
+                hits += found ? 1 : 0;
+            }
+        }
+    }
+    if (lane == 0 && pairs) {
+        atomicAdd(&counts[0], hits);
+        atomicAdd(&counts[1], pairs);
+    }
+}
+
 } // namespace
+
+// whether g has the local structure the locality layout exploits (sampled
+// clustering coefficient at least 0.1)
+bool vg_local_structure(vg_ctx *ctx, const vg_graph *g) {
+    if (g->nv < 3 || g->ne == 0) return false;
+    DevBuf<unsigned long long> counts(ctx, 2);
+    VG_CUDA(cudaMemsetAsync(counts.p, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    {
+        LaunchTimer lt(ctx);
+        k_cc_sample<<<CC_SAMPLE * 32 / 256, 256, 0, ctx->stream>>>(g->rowptr, g->tail, g->nv,
+                                                                 0xcc5eedULL, counts.p);
+    }
+    VG_CHECK_LAUNCH();
+    unsigned long long *h = (unsigned long long *)vg_pinned(ctx, 2 * sizeof(unsigned long long));
+    VG_CUDA(cudaMemcpyAsync(h, counts.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    vg_sync(ctx);
+    return h[1] > 0 && (double)h[0] >= 0.1 * (double)h[1];
+}
 
 int64_t vg_exclusive_scan_i64(vg_ctx *ctx, int64_t *data, int64_t n);
 

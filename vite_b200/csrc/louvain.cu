@@ -26,17 +26,26 @@ constexpr int NCLS = 5;
 // 4: above (CTA, table in global scratch)
 constexpr int TMAX = 16;
 constexpr int TB = 256;
-constexpr int WT_MAXDEG = 512;
+#ifndef VG_WT_MAXDEG
+#define VG_WT_MAXDEG 512
+#endif
+#ifndef VG_CT_MAXDEG
+#define VG_CT_MAXDEG 4096
+#endif
+#ifndef VG_T32
+#define VG_T32 1
+#endif
+constexpr int WT_MAXDEG = VG_WT_MAXDEG;
 constexpr int WT_CAP = 1024;
 constexpr int WT_WARPS = 4;
-constexpr int CT_MAXDEG = 4096;
+constexpr int CT_MAXDEG = VG_CT_MAXDEG;
 constexpr int CT_CAP = 8192;
 constexpr int CT_THREADS = 256;
 constexpr int32_t EMPTY = -1;
 
 __host__ __device__ __forceinline__ int degree_class(int64_t d) {
     if (d <= TMAX) return 0;
-    if (d <= 32) return 1;
+    if (VG_T32 && d <= 32) return 1;
     if (d <= WT_MAXDEG) return 2;
     if (d <= CT_MAXDEG) return 3;
     return 4;

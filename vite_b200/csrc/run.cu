@@ -80,7 +80,7 @@ extern "C" vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g0, const vg_ru
         vg_graph *cur = &view;
         VG_REQUIRE(rp->layout >= 0 && rp->layout <= 2, "layout must be 0, 1 or 2");
         double layout_s = 0.0;
-        if (!g0->ref && (rp->layout == 1 || (rp->layout == 2 && g0->nv >= (1 << 18)))) {
+        if (vg_auto_layout(ctx, g0, rp->layout)) {
             EventTimer tl(ctx->stream);
             DevBuf<int32_t> order;
             vg_bfs_order(ctx, g0, order);

@@ -148,6 +148,14 @@ vg_graph *vg_remove_layout(vg_ctx *ctx, const vg_graph *g);
 void vg_download_comm_ref(vg_ctx *ctx, const vg_graph *g, const int32_t *comm, int64_t *out);
 void vg_download_vals_ref(vg_ctx *ctx, const vg_graph *g, const int32_t *x, int64_t *out);
 void vg_ref_to_pos_inplace(vg_ctx *ctx, const vg_graph *g, int32_t *x, bool are_ids);
+// whether the locality layout pays for g (sampled clustering coefficient)
+bool vg_local_structure(vg_ctx *ctx, const vg_graph *g);
+// layout mode 2 (automatic): graphs of at least 2^18 vertices with local structure
+inline bool vg_auto_layout(vg_ctx *ctx, const vg_graph *g, int mode) {
+    if (g->ref || mode == 0) return false;
+    if (mode == 1) return true;
+    return g->nv >= (1 << 18) && vg_local_structure(ctx, g);
+}
 
 void vg_graph_release(vg_ctx *ctx, vg_graph *g);
 // the graph takes ownership of the three arrays
