@@ -168,3 +168,19 @@ def test_batch_rejects_what_it_does_not_run(ctx):
             b.submit(g)
     g.free()
     empty.free()
+
+
+def test_batch_captured_and_direct_iterations_agree(ctx):
+    # without profiling the batch replays captured CUDA graphs of one iteration;
+    # with it, every launch is issued directly: both give the same results
+    gs = mixed_unit(ctx)[:4]
+    graph_path = ctx.run_batch(gs, want_comm=True)
+    ctx.profile(True, reset=True)
+    try:
+        direct = ctx.run_batch(gs, want_comm=True)
+    finally:
+        ctx.profile(False, reset=True)
+    for a, b in zip(graph_path, direct):
+        assert_same(a, b, exact=True)
+    for g in gs:
+        g.free()

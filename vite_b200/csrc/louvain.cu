@@ -941,7 +941,11 @@ struct BatchDecide {
     int32_t *live_count;   // graphs still iterating after this iteration
     int32_t iter;
     int32_t past_idx;
+    const int32_t *iter_dev; // when set, the iteration number is read here (graph replays)
 };
+
+// iteration counter of a captured batch iteration
+__global__ void k_iter_inc(int32_t *__restrict__ it) { *it += 1; }
 
 // final reduction and the ABS_MOD_PER_ITER modularity (louvain.cpp:2518-2524),
 // one block per segment. One graph: out = {Q, frozen, le, la2}; a batch: the
@@ -972,7 +976,7 @@ __global__ void __launch_bounds__(SEG_FINAL) k_mod_seg(const double *__restrict_
                 out[2] = le;
                 out[3] = la2;
             } else {
-                bd.iters[j] = bd.iter;
+                bd.iters[j] = bd.iter_dev ? *bd.iter_dev : bd.iter;
                 if (__dsub_rn(m, bd.prev_mod[j]) < bd.thresh[j]) {
                     bd.done[j] = 1;
                     bd.resbuf[j] = (int8_t)bd.past_idx;
@@ -1562,14 +1566,12 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
     VG_CUDA(cudaMemsetAsync(resbuf.p, 0, J, ctx->stream));
     int32_t *hlive = (int32_t *)vg_pinned(ctx, sizeof(int32_t));
     int32_t *bufs[3] = {B0.p, B1.p, B2.p};
-    int pi = 0; // bufs[pi] = past, bufs[pi+1] = curr, bufs[pi+2] = target
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    if (sweep_ms) {
-        VG_CUDA(cudaEventCreate(&ev0));
-        VG_CUDA(cudaEventCreate(&ev1));
-        *sweep_ms = 0.0;
-    }
-    for (int32_t it = 1;; it++) {
+    DevBuf<int32_t> iter_dev(ctx, 1);
+    VG_CUDA(cudaMemsetAsync(iter_dev.p, 0, sizeof(int32_t), ctx->stream));
+    // one iteration with bufs[pi] = past, bufs[pi+1] = curr, bufs[pi+2] = target; the
+    // iteration number is `it`, or read from iter_dev after k_iter_inc when `graph`
+    auto enqueue = [&](int pi, int32_t it, bool graph, cudaEvent_t e0, cudaEvent_t e1) {
+        if (graph) k_iter_inc<<<1, 1, 0, ctx->stream>>>(iter_dev.p);
         SweepArgs a{};
         a.rowptr = U->rowptr;
         a.tail = U->tail;
@@ -1588,9 +1590,9 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
         a.jconst = jconst.p;
         a.jdone = done.p;
         VG_CUDA(cudaMemsetAsync(live.p, 0, sizeof(int32_t), ctx->stream));
-        if (ev0) VG_CUDA(cudaEventRecord(ev0, ctx->stream));
+        if (e0) VG_CUDA(cudaEventRecord(e0, ctx->stream));
         sweep_color(ctx, a, bk, 0, gt, true, nv);
-        if (ev1) VG_CUDA(cudaEventRecord(ev1, ctx->stream));
+        if (e1) VG_CUDA(cudaEventRecord(e1, ctx->stream));
         {
             LaunchTimer lt(ctx);
             k_apply_seg<<<agrid, SEG_THREADS, 0, ctx->stream>>>(seg.voff.p, seg.cb.p, J, seg.C,
@@ -1608,6 +1610,7 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
         bd.live_count = live.p;
         bd.iter = it;
         bd.past_idx = pi;
+        bd.iter_dev = graph ? iter_dev.p : nullptr;
         {
             LaunchTimer lt(ctx);
             k_mod_seg<<<(int)std::min<int64_t>(J, 65535), SEG_FINAL, 0, ctx->stream>>>(
@@ -1615,14 +1618,64 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
         }
         VG_CHECK_LAUNCH();
         VG_CUDA(cudaMemcpyAsync(hlive, live.p, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-        vg_sync(ctx);
-        if (ev0) {
-            float ms = 0.f;
-            VG_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-            *sweep_ms += ms;
+    };
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (sweep_ms) *sweep_ms = 0.0;
+    if (!ctx->profile) {
+        // captured iterations: three graphs (one per rotation of the community
+        // buffers) replayed in turn, one launch and one 4-byte read-back per iteration
+        cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+        int64_t per_iter = 0;
+        auto destroy = [&] {
+            for (auto &e : exec)
+                if (e) cudaGraphExecDestroy(e);
+        };
+        try {
+            for (int pi = 0; pi < 3; pi++) {
+                const int64_t l0 = ctx->profile_launches;
+                cudaGraph_t gr = nullptr;
+                VG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+                try {
+                    enqueue(pi, 0, true, nullptr, nullptr);
+                } catch (...) {
+                    cudaStreamEndCapture(ctx->stream, &gr);
+                    if (gr) cudaGraphDestroy(gr);
+                    throw;
+                }
+                VG_CUDA(cudaStreamEndCapture(ctx->stream, &gr));
+                const cudaError_t e = cudaGraphInstantiate(&exec[pi], gr, 0);
+                cudaGraphDestroy(gr);
+                VG_CUDA(e);
+                per_iter = ctx->profile_launches - l0 + 1; // + k_iter_inc
+                ctx->profile_launches = l0;
+            }
+            int pi = 0;
+            for (;;) {
+                VG_CUDA(cudaGraphLaunch(exec[pi], ctx->stream));
+                ctx->profile_launches += per_iter;
+                pi = (pi + 1) % 3;
+                vg_sync(ctx);
+                if (*hlive == 0) break;
+            }
+        } catch (...) {
+            destroy();
+            throw;
         }
-        if (*hlive == 0) break;
-        pi = (pi + 1) % 3; // past <- curr <- target <- past (louvain.cpp:565-570)
+        destroy();
+    } else {
+        VG_CUDA(cudaEventCreate(&ev0));
+        VG_CUDA(cudaEventCreate(&ev1));
+        for (int32_t it = 1;; it++) {
+            const int pi = (it - 1) % 3; // past <- curr <- target <- past (louvain.cpp:565-570)
+            enqueue(pi, it, false, sweep_ms ? ev0 : nullptr, sweep_ms ? ev1 : nullptr);
+            vg_sync(ctx);
+            if (sweep_ms) {
+                float ms = 0.f;
+                VG_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+                *sweep_ms += ms;
+            }
+            if (*hlive == 0) break;
+        }
     }
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
