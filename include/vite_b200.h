@@ -229,6 +229,21 @@ vg_status vg_batch_result(vg_batch *b, int64_t job, vg_level_stat *levels, int32
 vg_status vg_batch_forget(vg_batch *b, int64_t job);
 vg_status vg_batch_get_stats(vg_batch *b, vg_batch_stats *out);
 
+/* --- ground-truth comparison ------------------------------------------------- */
+
+/* compare_communities + compute_gini_coeff (compare.cpp:58-318): c1 is the truth
+ * (graphClustering -g), c2 the computed communities, both n labels in
+ * [0, 2^31 - 1); the number of communities of each is its largest label + 1.
+ * Pair counts over all vertex pairs, precision, recall, F-score and the Gini
+ * coefficient of each vector's community sizes, as the reference prints them. */
+typedef struct vg_compare_stats {
+    int64_t n, nc1, nc2;
+    int64_t same_same, same_diff, diff_same; /* true positives, false negatives, false positives */
+    double precision, recall, fscore, gini1, gini2;
+} vg_compare_stats;
+vg_status vg_compare_communities(vg_ctx *ctx, int64_t n, const int64_t *c1, const int64_t *c2,
+                                 vg_compare_stats *out);
+
 /* --- generators --------------------------------------------------------------- */
 
 /* generateInMemGraph for one rank (distgraph.cpp:391-407, 412-983): n points

@@ -902,3 +902,88 @@ int vo_run(const vo_graph *g0, const vo_run_params *rp, int max_levels, int64_t 
     vo_graph_free(&cur);
     return nrec;
 }
+
+/* ------------------------------------------------------------------------------
+ * compare_communities (compare.cpp:58-285) with its per-community pair loops, and
+ * compute_gini_coeff (compare.cpp:287-318).
+ */
+static int vo_cmp_i64(const void *a, const void *b) {
+    const int64_t x = *(const int64_t *)a, y = *(const int64_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+static double vo_gini(int64_t *size, int numColors) {
+    qsort(size, (size_t)numColors, sizeof(int64_t), vo_cmp_i64);
+    double numFunc = 0.0, denFunc = 0.0;
+    for (int64_t i = 0; i < numColors; i++) {
+        numFunc = numFunc + (double)((i + 1) * size[i]);
+        denFunc = denFunc + (double)size[i];
+    }
+    return ((2 * numFunc) / (numColors * denFunc)) - ((double)(numColors + 1) / (double)numColors);
+}
+
+/* community CSR of labels c: ptr[nc + 1], idx[n] (compare.cpp:97-141), sizes[nc] */
+static int vo_comm_csr(int64_t n, const int64_t *c, int64_t nc, int64_t **ptr, int64_t **idx,
+                       int64_t **sizes) {
+    int64_t *p = calloc((size_t)nc + 1, sizeof(int64_t));
+    int64_t *x = malloc(sizeof(int64_t) * (size_t)n);
+    int64_t *s = malloc(sizeof(int64_t) * (size_t)nc);
+    int64_t *fill = calloc((size_t)nc, sizeof(int64_t));
+    if (!p || !x || !s || !fill) {
+        free(p); free(x); free(s); free(fill);
+        return -1;
+    }
+    for (int64_t i = 0; i < n; i++) p[c[i] + 1]++;
+    for (int64_t k = 0; k < nc; k++) s[k] = p[k + 1];
+    for (int64_t k = 0; k < nc; k++) p[k + 1] += p[k];
+    for (int64_t i = 0; i < n; i++) x[p[c[i]] + fill[c[i]]++] = i;
+    free(fill);
+    *ptr = p;
+    *idx = x;
+    *sizes = s;
+    return 0;
+}
+
+int vo_compare(int64_t n, const int64_t *c1, const int64_t *c2, vo_compare_stats *out) {
+    if (n <= 0) return -1;
+    int64_t nc1 = -1, nc2 = -1;
+    for (int64_t i = 0; i < n; i++) {
+        if (c1[i] < 0 || c2[i] < 0) return -1;
+        if (c1[i] > nc1) nc1 = c1[i];
+        if (c2[i] > nc2) nc2 = c2[i];
+    }
+    nc1++;
+    nc2++;
+    int64_t *p1, *x1, *s1, *p2, *x2, *s2;
+    if (vo_comm_csr(n, c1, nc1, &p1, &x1, &s1)) return -1;
+    if (vo_comm_csr(n, c2, nc2, &p2, &x2, &s2)) {
+        free(p1); free(x1); free(s1);
+        return -1;
+    }
+    int64_t ss = 0, sd = 0, ds = 0, agree = 0;
+    for (int64_t ci = 0; ci < nc1; ci++)
+        for (int64_t i = p1[ci]; i < p1[ci + 1]; i++)
+            for (int64_t j = i + 1; j < p1[ci + 1]; j++) {
+                if (c2[x1[i]] == c2[x1[j]]) ss++;
+                else sd++;
+            }
+    for (int64_t ci = 0; ci < nc2; ci++)
+        for (int64_t i = p2[ci]; i < p2[ci + 1]; i++)
+            for (int64_t j = i + 1; j < p2[ci + 1]; j++) {
+                if (c1[x2[i]] == c1[x2[j]]) agree++;
+                else ds++;
+            }
+    out->n = n;
+    out->nc1 = nc1;
+    out->nc2 = nc2;
+    out->same_same = ss;
+    out->same_diff = sd;
+    out->diff_same = ds;
+    out->precision = (double)ss / (double)(ss + ds);
+    out->recall = (double)ss / (double)(ss + sd);
+    out->fscore = 2.0 * ((out->precision * out->recall) / (out->precision + out->recall));
+    out->gini1 = vo_gini(s1, (int)nc1);
+    out->gini2 = vo_gini(s2, (int)nc2);
+    free(p1); free(x1); free(s1); free(p2); free(x2); free(s2);
+    return agree == ss ? 0 : -2;
+}

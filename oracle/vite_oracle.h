@@ -94,6 +94,13 @@ int vo_run(const vo_graph *g0, const vo_run_params *rp, int max_levels, int64_t 
            int64_t *level_ne, int *level_iters, double *level_mod, int64_t *level_colors,
            double *seconds_out);
 
+/* compare_communities + compute_gini_coeff (compare.cpp:58-318): c1 the truth. */
+typedef struct vo_compare_stats {
+    int64_t n, nc1, nc2, same_same, same_diff, diff_same;
+    double precision, recall, fscore, gini1, gini2;
+} vo_compare_stats;
+int vo_compare(int64_t n, const int64_t *c1, const int64_t *c2, vo_compare_stats *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -83,6 +83,7 @@ def lib():
         L.vo_rebuild.argtypes = [gp, _i64p, gp]
         L.vo_run.argtypes = [gp, C.POINTER(_VoRun), C.c_int, _i64p, _i64p,
                              C.POINTER(C.c_int), _f64p, _i64p, _f64p]
+        L.vo_compare.argtypes = [C.c_int64, _i64p, _i64p, C.POINTER(CompareStats)]
         _lib = L
     return _lib
 
@@ -203,6 +204,28 @@ def color(g: Graph, n_hash: int, target_percent: int = 70, single: bool = False)
 
 def color_hash(a: int, seed: int) -> int:
     return int(lib().vo_color_hash(a & 0xFFFFFFFF, seed & 0xFFFFFFFF))
+
+
+class CompareStats(C.Structure):
+    _fields_ = [("n", C.c_int64), ("nc1", C.c_int64), ("nc2", C.c_int64),
+                ("same_same", C.c_int64), ("same_diff", C.c_int64), ("diff_same", C.c_int64),
+                ("precision", C.c_double), ("recall", C.c_double), ("fscore", C.c_double),
+                ("gini1", C.c_double), ("gini2", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def compare(truth: np.ndarray, found: np.ndarray) -> dict:
+    """compare_communities (compare.cpp:58-318): pair counts, precision, recall,
+    F-score and Gini coefficients of two community vectors (truth first)."""
+    a = np.ascontiguousarray(truth, dtype=np.int64)
+    b = np.ascontiguousarray(found, dtype=np.int64)
+    st = CompareStats()
+    rc = lib().vo_compare(len(a), a.ctypes.data_as(_i64p), b.ctypes.data_as(_i64p), C.byref(st))
+    if rc != 0:
+        raise ValueError(f"vo_compare failed ({rc})")
+    return st.as_dict()
 
 
 def rebuild(g: Graph, cvect: np.ndarray) -> Graph:

@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = [
     "vg_generate_rgg", "vg_generate_ba", "vg_generate_er", "vg_graph_reweight",
     "vg_graph_reorder", "vg_vertex_degree_noalloc",
     "vg_batch_create", "vg_batch_destroy", "vg_batch_submit", "vg_batch_step", "vg_batch_poll",
-    "vg_batch_result", "vg_batch_forget", "vg_batch_get_stats",
+    "vg_batch_result", "vg_batch_forget", "vg_batch_get_stats", "vg_compare_communities",
 ]
 
 VG_BATCH_TAKE = 1
@@ -68,6 +68,16 @@ class LevelStat(C.Structure):
                 ("seconds_color", C.c_double), ("seconds_phase", C.c_double),
                 ("seconds_sweep", C.c_double), ("seconds_rebuild", C.c_double),
                 ("edges_swept", C.c_int64), ("seconds_layout", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class CompareStats(C.Structure):
+    _fields_ = [("n", C.c_int64), ("nc1", C.c_int64), ("nc2", C.c_int64),
+                ("same_same", C.c_int64), ("same_diff", C.c_int64), ("diff_same", C.c_int64),
+                ("precision", C.c_double), ("recall", C.c_double), ("fscore", C.c_double),
+                ("gini1", C.c_double), ("gini2", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -138,6 +148,7 @@ def lib() -> C.CDLL:
                                       C.POINTER(C.c_int32), _i64p]
         L.vg_batch_forget.argtypes = [vp, C.c_int64]
         L.vg_batch_get_stats.argtypes = [vp, C.POINTER(BatchStats)]
+        L.vg_compare_communities.argtypes = [vp, C.c_int64, _i64p, _i64p, C.POINTER(CompareStats)]
         for name in EXPORTED_SYMBOLS:
             if name not in ("vg_last_error", "vg_ctx_bytes_in_use"):
                 getattr(L, name).restype = C.c_int
@@ -357,6 +368,18 @@ class Context:
         self._check(lib().vg_louvain_run(self.handle, g.handle, C.byref(p), stats, max_levels,
                                          C.byref(n), _ptr(comm)))
         return Levels([stats[i].as_dict() for i in range(min(n.value, max_levels))], comm)
+
+    def compare_communities(self, truth: np.ndarray, found: np.ndarray) -> dict:
+        """compare_communities (compare.cpp:58-318) on the device: pair counts,
+        precision, recall, F-score and Gini coefficients (truth first)."""
+        a = np.ascontiguousarray(truth, dtype=np.int64)
+        b = np.ascontiguousarray(found, dtype=np.int64)
+        if len(a) != len(b):
+            raise VgError(VG_ERR_ARG, "both community vectors need one label per vertex")
+        st = CompareStats()
+        self._check(lib().vg_compare_communities(self.handle, len(a), _ptr(a), _ptr(b),
+                                                 C.byref(st)))
+        return st.as_dict()
 
     def batch(self, budget: int = 0) -> "Batch":
         return Batch(self, budget)

@@ -133,8 +133,14 @@ void compose(std::vector<GraphElem> &commAll, const CommunityVector &cvect, int 
 int main(int argc, char *argv[]) {
     const Options o = parse(argc, argv);
     const int me = 0, nprocs = 1;
-    if (o.compareCommunities)
-        std::cout << "Ground-truth comparison (-g) is not part of vite-b200; communities are still computed." << std::endl;
+    // the ground truth, in LFR's "vertex community" format (main.cpp:119-138)
+    std::vector<GraphElem> commGroundTruth;
+    if (o.compareCommunities) {
+        const double tg1 = now();
+        loadGroundTruthFile(commGroundTruth, o.groundTruthFileName, o.isGroundTruthZeroBased);
+        std::cout << "Time taken to load ground truth file (" << o.groundTruthFileName
+                  << "): " << (now() - tg1) << std::endl;
+    }
     const double td0 = now();
     DistGraph *dg = nullptr;
     if (o.generateGraph)
@@ -164,7 +170,8 @@ int main(int argc, char *argv[]) {
     size_t ssz = 0, rsz = 0;
     const GraphElem nv = dg->getTotalNumVertices();
     std::vector<GraphElem> commAll;
-    if (o.outputFiles) commAll.assign(nv, -1);
+    const bool keepComm = o.outputFiles || o.compareCommunities; // main.cpp:236
+    if (keepComm) commAll.assign(nv, -1);
     GraphElem teps = 0;
     const bool et = o.earlyTerm;
     const int ty = o.ETType;
@@ -210,7 +217,7 @@ int main(int argc, char *argv[]) {
         ptotal += t0 - t1;
         ctime += t0 - t1;
         if ((currMod - prevMod) > threshold) {
-            if (o.outputFiles) compose(commAll, cvect, phase);
+            if (keepComm) compose(commAll, cvect, phase);
             if (!o.runOnePhase) {
                 const double t3 = now();
                 distbuildNextLevelGraph(nprocs, me, dg, ssz, rsz, ssizes, rsizes, svdata, rvdata, cvect);
@@ -265,6 +272,8 @@ int main(int argc, char *argv[]) {
         std::cout << "Saved community information (" << commAll.size() << " vertices)  on file: "
                   << outFileName << std::endl;
     }
+    // compare the computed communities with the ground truth (main.cpp:574-581)
+    if (o.compareCommunities) compare_communities(commGroundTruth, commAll);
     delete dg;
     return 0;
 }

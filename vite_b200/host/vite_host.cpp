@@ -6,8 +6,10 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <fstream>
 #include <iostream>
 #include <mutex>
+#include <sstream>
 
 namespace {
 
@@ -347,4 +349,59 @@ void generateInMemGraph(int rank, int nprocs, DistGraph *&dg, GraphElem nv,
         writeGraph(rank, nprocs, dg, unused, fileOut);
         std::cout << "Written binary file: " << fileOut << std::endl;
     }
+}
+
+// ---------------------------------------------------------------------------------------
+// ground truth
+
+void loadGroundTruthFile(std::vector<GraphElem> &commGroundTruth,
+                         std::string const &groundTruthFileName, bool isGroundTruthZeroBased) {
+    std::ifstream ifs(groundTruthFileName.c_str(), std::ifstream::in);
+    if (!ifs) {
+        std::cerr << "Error opening ground truth file: " << groundTruthFileName << std::endl;
+        exit(EXIT_FAILURE);
+    }
+    std::string line;
+    while (std::getline(ifs, line)) {
+        GraphElem v = -1, comm_id = -1;
+        std::istringstream iss(line);
+        iss >> v >> comm_id;
+        if (!isGroundTruthZeroBased) comm_id--;
+        commGroundTruth.push_back(comm_id);
+    }
+    std::cout << "Loaded ground-truth file: " << groundTruthFileName
+              << ", containing community information for " << commGroundTruth.size()
+              << " vertices." << std::endl;
+}
+
+void compare_communities(std::vector<GraphElem> const &C1, std::vector<GraphElem> const &C2) {
+    if (C1.empty() || C1.size() != C2.size()) {
+        std::cerr << "compare_communities: the truth has " << C1.size()
+                  << " vertices and the communities " << C2.size() << std::endl;
+        exit(EXIT_FAILURE);
+    }
+    vg_compare_stats st;
+    check(vg_compare_communities(vite_ctx(), (int64_t)C1.size(), C1.data(), C2.data(), &st),
+          "vg_compare_communities");
+    std::cout << "Number of unique communities in C1 = " << st.nc1 << ", and C2 = " << st.nc2
+              << std::endl;
+    std::cout << "*******************************************" << std::endl;
+    std::cout << "Communities comparison statistics:" << std::endl;
+    std::cout << "*******************************************" << std::endl;
+    std::cout << "|C1| (truth)       : " << st.n << std::endl;
+    std::cout << "#communities in C1 : " << st.nc1 << std::endl;
+    std::cout << "|C2| (output)      : " << st.n << std::endl;
+    std::cout << "#communities in C2 : " << st.nc2 << std::endl;
+    std::cout << "-------------------------------------------" << std::endl;
+    std::cout << "Same-Same (True positive)  : " << st.same_same << std::endl;
+    std::cout << "Same-Diff (False negative) : " << st.same_diff << std::endl;
+    std::cout << "Diff-Same (False positive) : " << st.diff_same << std::endl;
+    std::cout << "-------------------------------------------" << std::endl;
+    std::cout << "Precision :  " << st.precision << " (" << (st.precision * 100) << ")" << std::endl;
+    std::cout << "Recall    :  " << st.recall << " (" << (st.recall * 100) << ")" << std::endl;
+    std::cout << "F-score   :  " << st.fscore << std::endl;
+    std::cout << "-------------------------------------------" << std::endl;
+    std::cout << "Gini coefficient, C1  :  " << st.gini1 << std::endl;
+    std::cout << "Gini coefficient, C2  :  " << st.gini2 << std::endl;
+    std::cout << "*******************************************" << std::endl;
 }

@@ -185,6 +185,15 @@ void distbuildNextLevelGraph(int nprocs, int me, DistGraph *&dg, const size_t &s
                              const std::vector<GraphElem> &svdata,
                              const std::vector<GraphElem> &rvdata, CommunityVector &cvect);
 
+// --- ground truth (louvain.hpp:201, compare.hpp) -------------------------------------
+// one "vertex community" pair per line (LFR format); ids shifted down by one unless
+// zero-based
+void loadGroundTruthFile(std::vector<GraphElem> &commGroundTruth,
+                         std::string const &groundTruthFileName, bool isGroundTruthZeroBased);
+// pair counts, precision, recall, F-score and Gini coefficients of C2 against the
+// truth C1, printed as the reference prints them; computed on the GPU
+void compare_communities(std::vector<GraphElem> const &C1, std::vector<GraphElem> const &C2);
+
 // --- graph input/output and generation (distgraph.hpp:109-119) -----------------------
 void loadDistGraphMPIIO(int me, int nprocs, int ranks_per_node, DistGraph *&dg,
                         std::string &fileName);
