@@ -77,6 +77,26 @@ def dist_env():
     return ws, rank, local
 
 
+def collectives(ws: int, device: str):
+    """The replica path's two collectives: a barrier, and the max of a per-rank time
+    (every rank runs its own graph; the job's time is the slowest rank's)."""
+    import torch
+    import torch.distributed as dist
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier, max_over_ranks
+
+
 def workload_config(n: int) -> dict:
     return {"workload": f"RGG n={n} (Vite generator: LCG seed 1, r(n) radius, distance weights) "
                         f"+{EXTRA_PERCENT:g}% extra edges U(0,1) seed {SEED}; full multi-level "
@@ -391,16 +411,7 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
-    def barrier():
-        if ws > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = collectives(ws, "cuda")
 
     ctx = vite_b200.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream)
