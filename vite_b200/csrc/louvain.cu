@@ -733,12 +733,25 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
 // ---------------------------------------------------------------------------------
 // init, degree, apply + modularity, swaps
 
-// distSumVertexDegree (louvain.cpp:2161-2186): each row summed in CSR order. A
-// warp takes 32 consecutive rows; a row of at most DEG_LONG entries is summed by
-// its own lane. A longer row: with integral weights every order gives the same
-// exact sum, so the warp adds it as a tree; otherwise one lane forms the left
-// fold, its loads issued eight at a time ahead of the ordered additions.
+// distSumVertexDegree (louvain.cpp:2161-2186): each row summed in CSR order, one
+// row per lane, its loads issued eight at a time ahead of the ordered additions.
+// With integral weights every order gives the same exact sum, so a warp adds the
+// rows longer than DEG_LONG together as trees (no lane waits on a hub row).
 constexpr int DEG_LONG = 64;
+
+__device__ __forceinline__ double row_fold(const double *__restrict__ w, int64_t e0, int64_t e1) {
+    double sum = 0.0;
+    int64_t k = e0;
+    for (; k + 8 <= e1; k += 8) {
+        double x[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) x[t] = w[k + t];
+#pragma unroll
+        for (int t = 0; t < 8; t++) sum = __dadd_rn(sum, x[t]);
+    }
+    for (; k < e1; k++) sum = __dadd_rn(sum, w[k]);
+    return sum;
+}
 
 __global__ void k_degree(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
                          int64_t nv, double *__restrict__ vdeg, int integral) {
@@ -754,36 +767,17 @@ __global__ void k_degree(const int64_t *__restrict__ rowptr, const double *__res
             e0 = rowptr[v];
             e1 = rowptr[v + 1];
         }
-        const bool lng = valid && e1 - e0 > DEG_LONG;
-        if (valid && !lng) {
-            double tw = 0.0;
-            for (int64_t k = e0; k < e1; k++) tw = __dadd_rn(tw, w[k]);
-            vdeg[v] = tw;
-        }
-        unsigned lm = __ballot_sync(full, lng);
+        const bool coop = integral && valid && e1 - e0 > DEG_LONG;
+        if (valid && !coop) vdeg[v] = row_fold(w, e0, e1);
+        unsigned lm = __ballot_sync(full, coop);
         while (lm) {
             const int src = __ffs(lm) - 1;
             lm &= lm - 1;
             const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
             double sum = 0.0;
-            if (integral) {
-                for (int64_t k = E0 + lane; k < E1; k += 32) sum = __dadd_rn(sum, w[k]);
+            for (int64_t k = E0 + lane; k < E1; k += 32) sum = __dadd_rn(sum, w[k]);
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) sum = __dadd_rn(sum, __shfl_xor_sync(full, sum, o));
-            } else {
-                if (lane == 0) {
-                    int64_t k = E0;
-                    for (; k + 8 <= E1; k += 8) {
-                        double x[8];
-#pragma unroll
-                        for (int t = 0; t < 8; t++) x[t] = w[k + t];
-#pragma unroll
-                        for (int t = 0; t < 8; t++) sum = __dadd_rn(sum, x[t]);
-                    }
-                    for (; k < E1; k++) sum = __dadd_rn(sum, w[k]);
-                }
-                sum = __shfl_sync(full, sum, 0);
-            }
+            for (int o = 16; o > 0; o >>= 1) sum = __dadd_rn(sum, __shfl_xor_sync(full, sum, o));
             if (lane == src) vdeg[v] = sum;
         }
     }
@@ -1142,6 +1136,52 @@ __global__ void k_bucket_count(const int64_t *__restrict__ rowptr, int64_t nv,
 
 // Each block reserves a range per bucket with one atomic and places its vertices
 // there (order inside a bucket follows the blocks' chunks).
+// Order-preserving placement for at most 32 buckets (the uncoloured sweep): a
+// block ranks each round of 256 vertices of its chunk with match_any inside a warp
+// and per-warp counts across warps, so every list keeps position order within a
+// chunk and the list kernels walk adjacent rows.
+constexpr int PLACE_THREADS = 256;
+
+__global__ void __launch_bounds__(PLACE_THREADS) k_bucket_place_ordered(
+    const int64_t *__restrict__ rowptr, int64_t nv, int nb, int64_t chunk,
+    int32_t *__restrict__ fill, int32_t *__restrict__ list) {
+    __shared__ int32_t cnt[PLACE_THREADS / 32][32];
+    __shared__ int32_t base[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    // block totals first: one global reservation per bucket and block
+    if (threadIdx.x < 32) base[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t b0 = blockIdx.x * chunk, b1 = min(nv, b0 + chunk);
+    int64_t d;
+    for (int64_t i = b0 + threadIdx.x; i < b1; i += PLACE_THREADS)
+        atomicAdd(&base[bucket_key(rowptr, i, nullptr, 1, &d)], 1);
+    __syncthreads();
+    if (threadIdx.x < nb) base[threadIdx.x] = base[threadIdx.x] ? atomicAdd(&fill[threadIdx.x], base[threadIdx.x]) : 0;
+    __syncthreads();
+    for (int64_t r0 = b0; r0 < b1; r0 += PLACE_THREADS) {
+        const int64_t i = r0 + threadIdx.x;
+        const bool valid = i < b1;
+        const int k = valid ? bucket_key(rowptr, i, nullptr, 1, &d) : 32 + lane;
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        if (lane < 32) cnt[warp][lane] = 0;
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) cnt[warp][k] = __popc(peers);
+        __syncthreads();
+        int off = 0;
+        if (valid)
+            for (int w = 0; w < warp; w++) off += cnt[w][k];
+        if (valid) list[base[k] + off + __popc(peers & lt)] = (int32_t)i;
+        __syncthreads();
+        if (threadIdx.x < nb) {
+            int tot = 0;
+            for (int w = 0; w < PLACE_THREADS / 32; w++) tot += cnt[w][threadIdx.x];
+            base[threadIdx.x] += tot;
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_bucket_place(const int64_t *__restrict__ rowptr, int64_t nv,
                                const int32_t *__restrict__ colors, int64_t numColor, int nb,
                                int64_t chunk, int32_t *__restrict__ fill,
@@ -1212,7 +1252,11 @@ static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors,
     VG_CUDA(cudaMemcpyAsync(counts.p, fill.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice,
                             ctx->stream));
     b.list.alloc(ctx, nv);
-    if (nv) {
+    if (nv && !colors && nb <= 32) {
+        LaunchTimer lt(ctx);
+        k_bucket_place_ordered<<<blocks, PLACE_THREADS, 0, ctx->stream>>>(g->rowptr, nv, (int)nb,
+                                                                          chunk, counts.p, b.list.p);
+    } else if (nv) {
         LaunchTimer lt(ctx);
         k_bucket_place<<<blocks, 256, 2 * sizeof(int32_t) * nb, ctx->stream>>>(
             g->rowptr, nv, colors, numColor, (int)nb, chunk, counts.p, b.list.p);
