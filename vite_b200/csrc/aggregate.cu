@@ -6,10 +6,10 @@
 //      (keys in reference order), so each row's entries can be copied as whole
 //      CSR rows, in the reference's (vertex, edge) order, into one segment;
 //   2. each segment is reduced by c2 with every sum a left fold in segment order,
-//      giving the reference's sums bit for bit: one warp per segment of at most
-//      256 entries folds them into a shared-memory hash table in order and sorts
-//      the distinct keys; the longer segments go through one stable radix sort of
-//      all their entries by (segment, c2) and each run is folded in order;
+//      giving the reference's sums bit for bit: one warp per segment folds its
+//      entries into a shared-memory hash table in order and sorts the distinct
+//      keys; segments with more than 256 distinct keys go through one stable radix
+//      sort of all their entries by (segment, c2) and each run is folded in order;
 //   3. the unique entries are compacted into the next CSR.
 #include "vg_internal.cuh"
 
@@ -145,13 +145,14 @@ __device__ void bitonic(uint64_t *sk, int n2, int t, int nt) {
         }
 }
 
-// One warp per segment of at most H_MAXL entries. The segment is read in chunks of
-// 32 entries; inside a chunk the lanes holding the same key elect the lowest as
-// leader, which adds its peers' weights in lane order onto the key's running sum
-// in a shared-memory table, so every sum is the left fold in segment order. Only
-// the distinct keys are then sorted: in registers across the warp when there are
-// at most 32 of them, else in shared memory. Longer segments are flagged.
-constexpr int H_MAXL = 256;
+// One warp per segment. The segment is read in chunks of 32 entries; inside a
+// chunk the lanes holding the same key elect the lowest as leader, which adds its
+// peers' weights in lane order onto the key's running sum in a shared-memory
+// table, so every sum is the left fold in segment order. Only the distinct keys
+// are then sorted: in registers across the warp when there are at most 32 of
+// them, else in shared memory. A segment with more than H_MAXU distinct keys is
+// flagged for the sorted path.
+constexpr int H_MAXU = 256;
 constexpr int H_CAP = 512;
 constexpr int H_WARPS = 8;
 constexpr int32_t H_EMPTY = -1;
@@ -159,7 +160,7 @@ constexpr int32_t H_EMPTY = -1;
 struct HashWarpSmem {
     int32_t keys[H_CAP];
     double vals[H_CAP];
-    uint64_t list[H_MAXL]; // (key << 32 | slot) of the distinct keys
+    uint64_t list[H_MAXU + 32]; // (key << 32 | slot) of the distinct keys
     double stage[32];
 };
 
@@ -175,20 +176,16 @@ __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t row = wg; row < nc; row += nw) {
         const int64_t b = rstart[row];
-        const int64_t L64 = rstart[row + 1] - b;
-        if (L64 > H_MAXL) {
-            if (lane == 0) flag[row] = 1;
-            continue;
-        }
-        const int L = (int)L64;
+        const int64_t L = rstart[row + 1] - b;
         int logcap = 5;
-        while ((1 << logcap) < 2 * L) logcap++;
-        const int cap = 1 << logcap;
+        while ((1 << logcap) < 2 * L && (1 << logcap) < H_CAP) logcap++;
+        const int cap = 1 << logcap; // > twice the distinct keys held (at most H_MAXU + 31)
         for (int s = lane; s < cap; s += 32) S.keys[s] = H_EMPTY;
         __syncwarp();
         int U = 0;
-        for (int base = 0; base < L; base += 32) {
-            const int i = base + lane;
+        bool over = false;
+        for (int64_t base = 0; base < L; base += 32) {
+            const int64_t i = base + lane;
             const bool has = i < L;
             int32_t k = -2 - lane; // distinct non-keys for idle lanes
             double w = 0.0;
@@ -230,6 +227,15 @@ __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
             if (fresh) S.list[U + __popc(fm & lt)] = ((uint64_t)(uint32_t)k << 32) | (uint32_t)slot;
             U += __popc(fm);
             __syncwarp();
+            if (U > H_MAXU) { // too many distinct keys for the table: the sorted path
+                over = true;
+                break;
+            }
+        }
+        if (over) {
+            if (lane == 0) flag[row] = 1;
+            __syncwarp();
+            continue;
         }
         if (U <= 32) {
             // bitonic network across the lanes on (key, sum)
@@ -279,7 +285,7 @@ __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
     }
 }
 
-// Segments longer than H_MAXL, all together: every entry becomes the key
+// Segments with more than H_MAXU distinct keys, all together: every entry becomes the key
 // (segment rank << kbits | neighbour key) with its index in the grouped arrays as
 // payload; one stable radix sort over all of them puts each (segment, key) run in
 // segment order, and the run is folded left to right.
@@ -525,7 +531,7 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
                         H_WARPS * sizeof(HashWarpSmem), ctx->stream>>>(
               nc, rstart.p, gk.p, gw.p, uk.p, uw.p, ucount.p, flag.p); }
         VG_CHECK_LAUNCH();
-        // segments longer than H_MAXL: one global stable sort
+        // segments with more than H_MAXU distinct keys: one global stable sort
         DevBuf<int64_t> bigidx(ctx, nc + 1), boff(ctx, nc + 1);
         const int64_t nbig = vg_exclusive_scan_i32_to_i64(ctx, flag.p, bigidx.p, nc);
         if (nbig > 0) {
