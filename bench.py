@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS, help=argparse.SUPPRESS)
     ap.add_argument("--skip-batched", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--skip-serving", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--check-reference", action="store_true",
+                    help="also run the reference on the full graph and compare every level")
     return ap.parse_args()
 
 
@@ -392,6 +394,45 @@ def run_serving(ctx, count: int) -> dict:
     }
 
 
+def check_reference_full(ctx, g, rp, ed, ours: list) -> dict:
+    """The reference (oracle/_ref, all host threads) on the full benchmark graph,
+    read from a Vite binary file: per-level vertices, entries, iterations and
+    modularity against ours, and the level-0 partitions compared with the device
+    ground-truth comparison (the reference as truth)."""
+    import struct
+
+    from oracle import vite_oracle as vo
+
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "rgg.bin")
+        with open(path, "wb") as f:  # Vite's binary layout: nv, ne, rowptr, Edge records
+            f.write(struct.pack("<qq", len(rp) - 1, len(ed)))
+            np.ascontiguousarray(rp, dtype="<i8").tofile(f)
+            ed.tofile(f)
+        rec = os.path.join(tmp, "ref.rec")
+        t0 = time.perf_counter()
+        vo.run_harness(["-f", path], rec, threads=threads, timeout=3600)
+        ref_s = time.perf_counter() - t0
+        r = vo.read_record(rec)
+    ref_levels = [lv for lv in r.levels if lv.level >= 0]
+    per = []
+    for a, b in zip(ours, ref_levels):
+        per.append({"nv": [a["nv"], b.nv], "ne": [a["ne"], b.ne], "iters": [a["iters"], b.iters],
+                    "modularity": [a["modularity"], b.mod],
+                    "rel_diff": abs(a["modularity"] - b.mod) / abs(b.mod)})
+    cv0, _, _ = ctx.louvain_phase(g, threshold=THRESHOLD)
+    cmp0 = ctx.compare_communities(ref_levels[0].cvect, cv0)
+    return {"reference": f"oracle/_ref/vite_ref_harness -f <graph> ({threads} threads), "
+                         f"{ref_s:.1f} s wall including the file read",
+            "levels": [len(ours), len(ref_levels)],
+            "max_rel_modularity_diff": max(p["rel_diff"] for p in per),
+            "final_modularity": [ours[-1]["modularity"], ref_levels[-1].mod],
+            "level0_partition_vs_reference": {k: cmp0[k] for k in ("nc1", "nc2", "precision",
+                                                                   "recall", "fscore")},
+            "per_level": per}
+
+
 def main() -> None:
     args = parse()
     ws, rank, local = dist_env()
@@ -538,6 +579,8 @@ def main() -> None:
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    if ws == 1 and args.check_reference:
+        line["check_reference"] = check_reference_full(ctx, g, rp_pin.numpy(), ed, last)
     if ws == 1 and not args.skip_batched:
         line["batched"] = run_batched(ctx, stream, args.batch_graphs)
     if ws == 1 and not args.skip_serving:
