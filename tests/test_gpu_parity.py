@@ -7,6 +7,7 @@ modularity must agree within REL_TOL relative (the reference's own OpenMP
 atomics and reductions already reorder those sums).
 """
 import hashlib
+import os
 
 import numpy as np
 import pytest
@@ -367,3 +368,26 @@ def test_large_rgg_properties(ctx):
     src = np.repeat(np.arange(n), np.diff(rp))
     both = (colors[src] >= 0) & (colors[tail] >= 0) & (src != tail)
     assert not np.any(colors[src][both] == colors[tail][both])
+
+
+@pytest.mark.skipif(not os.path.exists(vo.HARNESS), reason="reference build absent")
+@pytest.mark.parametrize("flags", [["-c", "8", "-t", "2", "-a", "0.25"], []])
+def test_ba_1m_matches_reference_every_level(ctx, tmp_path, flags):
+    """A preferential-attachment graph of 2^20 vertices (m = 8, unit weights: every sum is
+    exact), large enough for hub rows in the warp and CTA degree classes, run with the
+    config-3 heuristics and plain: each level bit-identical to the reference's own run
+    (all host threads)."""
+    g = ctx.generate_ba(1 << 20, 8, 4242)
+    rp, tail, w = g.download()
+    path = str(tmp_path / "ba.bin")
+    vo.write_vite_binary(path, vo.Graph(rp, tail, w))
+    rec = str(tmp_path / "ba.rec")
+    vo.run_harness(["-f", path, *flags], rec, threads=os.cpu_count() or 1, timeout=1800)
+    ref = [lv for lv in vo.read_record(rec).levels if lv.level >= 0]
+    res = ctx.run(g, want_comm=False, **vo.flags_to_kwargs(flags))
+    assert [(s["nv"], s["ne"], s["iters"]) for s in res.stats] == [(lv.nv, lv.ne, lv.iters) for lv in ref]
+    assert [float(s["modularity"]).hex() for s in res.stats] == [float(lv.mod).hex() for lv in ref]
+    if not flags:  # plain: the level-0 partition itself
+        cv, _, _ = ctx.louvain_phase(g)
+        np.testing.assert_array_equal(cv, ref[0].cvect)
+    g.free()
