@@ -37,8 +37,9 @@ __global__ void k_bfs_init(int64_t nv, uint64_t seed, int32_t *__restrict__ labe
 }
 
 // one level: vertices at distance step-1 claim their unlabeled neighbours. A warp
-// takes 32 consecutive vertices; a frontier row of at most 64 entries is scanned
-// by its own lane, a longer one by the whole warp.
+// takes 32 consecutive vertices and walks the frontier rows among them one at a
+// time, lane j on entry j, so a row's claims are issued together instead of as a
+// chain of dependent loads and compare-and-swaps.
 // unvisited vertices are found through the byte array of distances (255 =
 // unvisited), which stays in L2; the label's compare-and-swap settles races
 __device__ __forceinline__ unsigned long long bfs_claim(const int32_t *__restrict__ tail, int64_t e,
@@ -71,13 +72,10 @@ __global__ void k_bfs_step(const int64_t *__restrict__ rowptr, const int32_t *__
             e1 = rowptr[u + 1];
             lu = label[u];
         }
-        const bool lng = front && e1 - e0 > 64;
-        if (front && !lng)
-            for (int64_t e = e0; e < e1; e++) mine += bfs_claim(tail, e, lu, step, label, dist);
-        unsigned lm = __ballot_sync(full, lng);
-        while (lm) {
-            const int src = __ffs(lm) - 1;
-            lm &= lm - 1;
+        unsigned fm = __ballot_sync(full, front);
+        while (fm) {
+            const int src = __ffs(fm) - 1;
+            fm &= fm - 1;
             const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
             const int32_t L = __shfl_sync(full, lu, src);
             for (int64_t e = E0 + lane; e < E1; e += 32) mine += bfs_claim(tail, e, L, step, label, dist);
