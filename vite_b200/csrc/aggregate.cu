@@ -77,24 +77,25 @@ __global__ void k_group_copy(const int64_t *__restrict__ rowptr, const int32_t *
     }
 }
 
-// rows [offs[r], offs[r+1]) longer than LONG_ROW: their list and chunk counts
-__global__ void k_long_flags(const int64_t *__restrict__ offs, int64_t n, int32_t *__restrict__ flag) {
+// rows [offs[r], offs[r+1]) longer than LONG_ROW, in any order (each chunk writes
+// its own entries, so the order changes no result): list[s] = row, chunks[s] = its
+// chunk count; cnt[0] counts them. At most cap rows qualify (each has more than
+// LONG_ROW of the offs' entries); the guard keeps writes inside the lists anyway.
+__global__ void k_long_collect(const int64_t *__restrict__ offs, int64_t n, int64_t cap,
+                               int32_t *__restrict__ list, int64_t *__restrict__ chunks,
+                               int64_t *__restrict__ cnt) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
-         r += (int64_t)gridDim.x * blockDim.x)
-        flag[r] = offs[r + 1] - offs[r] > LONG_ROW ? 1 : 0;
-}
-
-__global__ void k_long_place(const int32_t *__restrict__ flag, const int64_t *__restrict__ idx,
-                             int64_t n, const int64_t *__restrict__ offs,
-                             int32_t *__restrict__ list, int64_t *__restrict__ nch) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
-         r += (int64_t)gridDim.x * blockDim.x)
-        if (flag[r]) {
-            list[idx[r]] = (int32_t)r;
-            nch[idx[r]] = (offs[r + 1] - offs[r] + COPY_CHUNK - 1) / COPY_CHUNK;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t len = offs[r + 1] - offs[r];
+        if (len > LONG_ROW) {
+            const int64_t s = (int64_t)atomicAdd((unsigned long long *)cnt, 1ULL);
+            if (s < cap) {
+                list[s] = (int32_t)r;
+                chunks[s] = (len + COPY_CHUNK - 1) / COPY_CHUNK;
+            }
         }
+    }
 }
-
 __device__ __forceinline__ int64_t chunk_owner(const int64_t *__restrict__ cb, int64_t n, int64_t c) {
     int64_t lo = 0, hi = n; // largest q with cb[q] <= c
     while (hi - lo > 1) {
@@ -109,8 +110,9 @@ __global__ void k_group_copy_long(const int64_t *__restrict__ rowptr, const int3
                                   const double *__restrict__ w, const int32_t *__restrict__ pos,
                                   const uint32_t *__restrict__ order, const int64_t *__restrict__ off,
                                   const int32_t *__restrict__ list, const int64_t *__restrict__ cb,
-                                  int64_t nl, int64_t nchunks, const int32_t *__restrict__ new_key,
+                                  const int64_t *__restrict__ cnt, const int32_t *__restrict__ new_key,
                                   int32_t *__restrict__ gk, double *__restrict__ gw) {
+    const int64_t nl = cnt[0], nchunks = cnt[1];
     for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
         const int64_t q = chunk_owner(cb, nl, c);
         const int64_t k = list[q];
@@ -296,40 +298,39 @@ __global__ void k_big_rowmap(int64_t nc, const int32_t *__restrict__ flag,
         if (flag[r]) big_row[bigidx[r]] = (int32_t)r;
 }
 
-__global__ void k_big_lengths(int64_t nc, const int32_t *__restrict__ flag,
-                              const int64_t *__restrict__ rstart, int64_t *__restrict__ len) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nc;
-         r += (int64_t)gridDim.x * blockDim.x)
-        len[r] = flag[r] ? rstart[r + 1] - rstart[r] : 0;
-}
-
 constexpr int BIG_CHUNK = 4096;
 
-__global__ void k_big_chunks(int64_t nbig, const int32_t *__restrict__ big_row,
-                             const int64_t *__restrict__ rstart, int64_t *__restrict__ nch) {
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nbig;
-         q += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t r = big_row[q];
-        nch[q] = (rstart[r + 1] - rstart[r] + BIG_CHUNK - 1) / BIG_CHUNK;
+// per segment r: its length and chunk count when flagged (more distinct keys than
+// the warp table holds), else 0
+__global__ void k_big_prep(int64_t nc, const int32_t *__restrict__ flag,
+                           const int64_t *__restrict__ rstart, int64_t *__restrict__ len,
+                           int64_t *__restrict__ chunks) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nc;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t L = flag[r] ? rstart[r + 1] - rstart[r] : 0;
+        len[r] = L;
+        chunks[r] = (L + BIG_CHUNK - 1) / BIG_CHUNK;
     }
 }
 
-// one block per chunk of BIG_CHUNK entries of a long segment
-__global__ void k_big_keys(int64_t nbig, const int64_t *__restrict__ cb, int64_t nchunks,
-                           const int32_t *__restrict__ big_row, const int64_t *__restrict__ rstart,
+// one block per chunk of BIG_CHUNK entries of a flagged segment; cb: exclusive
+// prefix of the chunk counts over all nc segments (unflagged ones hold none, so the
+// largest r with cb[r] <= c owns chunk c); q = bigidx[r] is the segment's rank
+// among the flagged ones and leads its sort key
+__global__ void k_big_keys(int64_t nc, const int64_t *__restrict__ cb, int64_t nchunks,
+                           const int64_t *__restrict__ bigidx, const int64_t *__restrict__ rstart,
                            const int64_t *__restrict__ boff, const int32_t *__restrict__ gk,
                            int kbits, uint64_t *__restrict__ K, uint32_t *__restrict__ V) {
     for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
-        int64_t lo = 0, hi = nbig; // largest q with cb[q] <= c
+        int64_t lo = 0, hi = nc;
         while (hi - lo > 1) {
             const int64_t mid = (lo + hi) >> 1;
             if (cb[mid] <= c) lo = mid;
             else hi = mid;
         }
-        const int64_t q = lo;
-        const int32_t r = big_row[q];
+        const int64_t r = lo, q = bigidx[r];
         const int64_t b = rstart[r], L = rstart[r + 1] - b, o = boff[r];
-        const int64_t i0 = (c - cb[q]) * BIG_CHUNK, i1 = min(i0 + BIG_CHUNK, L);
+        const int64_t i0 = (c - cb[r]) * BIG_CHUNK, i1 = min(i0 + BIG_CHUNK, L);
         for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
             K[o + i] = ((uint64_t)q << kbits) | (uint64_t)(uint32_t)gk[b + i];
             V[o + i] = (uint32_t)(b + i);
@@ -358,11 +359,13 @@ __global__ void k_big_rowfirst(const uint64_t *__restrict__ K, int64_t m, int kb
 // one thread per run: the run's bounds are known, so its weights are fetched
 // eight at a time ahead of the strictly ordered additions
 __global__ void k_big_fold(const uint64_t *__restrict__ K, const uint32_t *__restrict__ V, int64_t m,
-                           int kbits, int64_t nheads, const int64_t *__restrict__ headpos,
+                           int kbits, const int64_t *__restrict__ nheads_dev,
+                           const int64_t *__restrict__ headpos,
                            const int64_t *__restrict__ rowfirst, const int32_t *__restrict__ big_row,
                            const int64_t *__restrict__ rstart, const double *__restrict__ gw,
                            int32_t *__restrict__ uk, double *__restrict__ uw) {
     const uint64_t mask = ((uint64_t)1 << kbits) - 1;
+    const int64_t nheads = *nheads_dev;
     for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nheads;
          h += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i0 = headpos[h], i1 = h + 1 < nheads ? headpos[h + 1] : m;
@@ -385,8 +388,9 @@ __global__ void k_big_fold(const uint64_t *__restrict__ K, const uint32_t *__res
 }
 
 __global__ void k_big_counts(int64_t nbig, const int32_t *__restrict__ big_row,
-                             const int64_t *__restrict__ rowfirst, int64_t heads,
-                             int64_t *__restrict__ ucount) {
+                             const int64_t *__restrict__ rowfirst,
+                             const int64_t *__restrict__ heads_dev, int64_t *__restrict__ ucount) {
+    const int64_t heads = *heads_dev;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nbig;
          q += (int64_t)gridDim.x * blockDim.x)
         ucount[big_row[q]] = (q + 1 < nbig ? rowfirst[q + 1] : heads) - rowfirst[q];
@@ -412,9 +416,10 @@ __global__ void k_compact_rows(int64_t nc, const int64_t *__restrict__ rstart,
 
 __global__ void k_compact_long(const int64_t *__restrict__ rstart, const int64_t *__restrict__ rowptr,
                                const int32_t *__restrict__ list, const int64_t *__restrict__ cb,
-                               int64_t nl, int64_t nchunks, const int32_t *__restrict__ uk,
+                               const int64_t *__restrict__ cnt, const int32_t *__restrict__ uk,
                                const double *__restrict__ uw, const int32_t *__restrict__ key_to_pos,
                                int32_t *__restrict__ tail, double *__restrict__ w) {
+    const int64_t nl = cnt[0], nchunks = cnt[1];
     for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
         const int64_t q = chunk_owner(cb, nl, c);
         const int64_t row = list[q];
@@ -428,29 +433,31 @@ __global__ void k_compact_long(const int64_t *__restrict__ rstart, const int64_t
     }
 }
 
-// the rows of offs (n + 1 offsets) longer than LONG_ROW, with their chunk prefix
+// The rows of offs (n + 1 offsets, total entries) longer than LONG_ROW with the
+// exclusive prefix of their chunk counts, all stream-ordered: the counts stay on
+// the device (cnt[0] rows, cnt[1] chunks) for the chunk kernels to read. grid: the
+// blocks those kernels take (0 when no row can be long).
 struct LongRows {
     DevBuf<int32_t> list;
-    DevBuf<int64_t> cb;
-    int64_t n = 0, nch = 0;
+    DevBuf<int64_t> cb, cnt;
+    int grid = 0;
 };
 
-void long_rows(vg_ctx *ctx, const int64_t *offs, int64_t n, LongRows &L) {
-    if (n == 0) return;
-    DevBuf<int32_t> flag(ctx, n);
-    DevBuf<int64_t> idx(ctx, n);
+void long_rows(vg_ctx *ctx, const int64_t *offs, int64_t n, int64_t total, LongRows &L) {
+    const int64_t cap = total / (LONG_ROW + 1);
+    if (n == 0 || cap == 0) return;
+    L.list.alloc(ctx, cap);
+    L.cb.alloc(ctx, cap);
+    L.cnt.alloc(ctx, 2);
+    VG_CUDA(cudaMemsetAsync(L.cnt.p, 0, 2 * sizeof(int64_t), ctx->stream));
+    VG_CUDA(cudaMemsetAsync(L.cb.p, 0, cap * sizeof(int64_t), ctx->stream));
     { LaunchTimer lt(ctx);
-      k_long_flags<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(offs, n, flag.p); }
+      k_long_collect<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(offs, n, cap, L.list.p, L.cb.p,
+                                                                     L.cnt.p); }
     VG_CHECK_LAUNCH();
-    L.n = vg_exclusive_scan_i32_to_i64(ctx, flag.p, idx.p, n);
-    if (L.n == 0) return;
-    L.list.alloc(ctx, L.n);
-    L.cb.alloc(ctx, L.n + 1);
-    { LaunchTimer lt(ctx);
-      k_long_place<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(flag.p, idx.p, n, offs, L.list.p,
-                                                                  L.cb.p); }
-    VG_CHECK_LAUNCH();
-    L.nch = vg_exclusive_scan_i64(ctx, L.cb.p, L.n);
+    vg_scan_i64_async(ctx, L.cb.p, cap, L.cnt.p + 1);
+    // each long row has more than COPY_CHUNK entries: chunks <= total / COPY_CHUNK + rows
+    L.grid = (int)std::min<int64_t>(total / COPY_CHUNK + cap, 16LL * ctx->sm_count);
 }
 
 } // namespace
@@ -489,7 +496,7 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
           k_sorted_deg<<<grid, 256, 0, ctx->stream>>>(g->rowptr, pos, vorder.p, nv, off.p); }
         VG_CHECK_LAUNCH();
     }
-    vg_exclusive_scan_i64(ctx, off.p, nv + 1);
+    vg_scan_i64_async(ctx, off.p, nv + 1, nullptr);
     VG_CUDA(cudaMemcpyAsync(rstart.p + nc, &ne, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
     if (nv) {
         { LaunchTimer lt(ctx);
@@ -508,12 +515,12 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     VG_CHECK_LAUNCH();
     {
         LongRows L;
-        long_rows(ctx, off.p, nv, L);
-        if (L.nch) {
+        long_rows(ctx, off.p, nv, ne, L);
+        if (L.grid) {
             LaunchTimer lt(ctx);
-            k_group_copy_long<<<(int)std::min<int64_t>(L.nch, 16LL * ctx->sm_count), 256, 0,
-                                ctx->stream>>>(g->rowptr, g->tail, g->weight, pos, vorder.p, off.p,
-                                               L.list.p, L.cb.p, L.n, L.nch, new_key, gk.p, gw.p);
+            k_group_copy_long<<<L.grid, 256, 0, ctx->stream>>>(g->rowptr, g->tail, g->weight, pos,
+                                                               vorder.p, off.p, L.list.p, L.cb.p,
+                                                               L.cnt.p, new_key, gk.p, gw.p);
         }
         VG_CHECK_LAUNCH();
     }
@@ -531,15 +538,22 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
                         H_WARPS * sizeof(HashWarpSmem), ctx->stream>>>(
               nc, rstart.p, gk.p, gw.p, uk.p, uw.p, ucount.p, flag.p); }
         VG_CHECK_LAUNCH();
-        // segments with more than H_MAXU distinct keys: one global stable sort
-        DevBuf<int64_t> bigidx(ctx, nc + 1), boff(ctx, nc + 1);
-        const int64_t nbig = vg_exclusive_scan_i32_to_i64(ctx, flag.p, bigidx.p, nc);
+        // segments with more than H_MAXU distinct keys: one global stable sort. Their
+        // count, entries and chunks are scanned on the device and read back together.
+        DevBuf<int64_t> bigidx(ctx, nc), boff(ctx, nc), cb(ctx, nc), tot(ctx, 4);
+        { LaunchTimer lt(ctx);
+          k_big_prep<<<vg_grid(ctx, nc, 256), 256, 0, ctx->stream>>>(nc, flag.p, rstart.p, boff.p,
+                                                                     cb.p); }
+        VG_CHECK_LAUNCH();
+        vg_scan_i32_async(ctx, flag.p, bigidx.p, nc, tot.p);
+        vg_scan_i64_async(ctx, boff.p, nc, tot.p + 1);
+        vg_scan_i64_async(ctx, cb.p, nc, tot.p + 2);
+        int64_t *ht = (int64_t *)vg_pinned(ctx, 3 * sizeof(int64_t));
+        VG_CUDA(cudaMemcpyAsync(ht, tot.p, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        vg_sync(ctx);
+        const int64_t nbig = ht[0], m = ht[1], nch = ht[2];
         if (nbig > 0) {
-            { LaunchTimer lt(ctx);
-              k_big_lengths<<<vg_grid(ctx, nc, 256), 256, 0, ctx->stream>>>(nc, flag.p, rstart.p,
-                                                                            boff.p); }
-            VG_CHECK_LAUNCH();
-            const int64_t m = vg_exclusive_scan_i64(ctx, boff.p, nc);
             DevBuf<int32_t> big_row(ctx, nbig);
             { LaunchTimer lt(ctx);
               k_big_rowmap<<<vg_grid(ctx, nc, 256), 256, 0, ctx->stream>>>(nc, flag.p, bigidx.p,
@@ -550,41 +564,35 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
             VG_REQUIRE(kbits + qbits <= 64, "aggregation keys need %d bits", kbits + qbits);
             DevBuf<uint64_t> K(ctx, m);
             DevBuf<uint32_t> V(ctx, m);
-            {
-                DevBuf<int64_t> cb(ctx, nbig + 1);
-                { LaunchTimer lt(ctx);
-                  k_big_chunks<<<vg_grid(ctx, nbig, 256), 256, 0, ctx->stream>>>(nbig, big_row.p,
-                                                                                rstart.p, cb.p); }
-                VG_CHECK_LAUNCH();
-                const int64_t nch = vg_exclusive_scan_i64(ctx, cb.p, nbig);
-                { LaunchTimer lt(ctx);
-                  k_big_keys<<<(int)std::min<int64_t>(nch, 16LL * ctx->sm_count), 256, 0,
-                               ctx->stream>>>(nbig, cb.p, nch, big_row.p, rstart.p, boff.p, gk.p,
-                                              kbits, K.p, V.p); }
-                VG_CHECK_LAUNCH();
-            }
+            { LaunchTimer lt(ctx);
+              k_big_keys<<<(int)std::min<int64_t>(nch, 16LL * ctx->sm_count), 256, 0,
+                           ctx->stream>>>(nc, cb.p, nch, bigidx.p, rstart.p, boff.p, gk.p, kbits,
+                                          K.p, V.p); }
+            VG_CHECK_LAUNCH();
+            cb.release();
             vg_radix_sort_pairs(ctx, K.p, V.p, m, kbits + qbits);
+            // runs of equal (segment, key): their count stays on the device (tot[3]);
+            // headpos is sized by its bound m
             DevBuf<int32_t> heads(ctx, m);
-            DevBuf<int64_t> hr(ctx, m), rowfirst(ctx, nbig);
+            DevBuf<int64_t> hr(ctx, m), rowfirst(ctx, nbig), headpos(ctx, m);
             { LaunchTimer lt(ctx);
               k_big_heads<<<vg_grid(ctx, m, 256), 256, 0, ctx->stream>>>(K.p, m, heads.p); }
             VG_CHECK_LAUNCH();
-            const int64_t nheads = vg_exclusive_scan_i32_to_i64(ctx, heads.p, hr.p, m);
+            vg_scan_i32_async(ctx, heads.p, hr.p, m, tot.p + 3);
             heads.release();
-            DevBuf<int64_t> headpos(ctx, nheads);
             { LaunchTimer lt(ctx);
               k_big_rowfirst<<<vg_grid(ctx, m, 256), 256, 0, ctx->stream>>>(K.p, m, kbits, hr.p,
                                                                             rowfirst.p, headpos.p); }
             VG_CHECK_LAUNCH();
             hr.release();
             { LaunchTimer lt(ctx);
-              k_big_fold<<<vg_grid(ctx, nheads, 128), 128, 0, ctx->stream>>>(
-                  K.p, V.p, m, kbits, nheads, headpos.p, rowfirst.p, big_row.p, rstart.p, gw.p,
+              k_big_fold<<<vg_grid(ctx, m, 128), 128, 0, ctx->stream>>>(
+                  K.p, V.p, m, kbits, tot.p + 3, headpos.p, rowfirst.p, big_row.p, rstart.p, gw.p,
                   uk.p, uw.p); }
             VG_CHECK_LAUNCH();
             { LaunchTimer lt(ctx);
               k_big_counts<<<vg_grid(ctx, nbig, 256), 256, 0, ctx->stream>>>(
-                  nbig, big_row.p, rowfirst.p, nheads, ucount.p); }
+                  nbig, big_row.p, rowfirst.p, tot.p + 3, ucount.p); }
             VG_CHECK_LAUNCH();
         }
     }
@@ -602,15 +610,14 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     VG_CHECK_LAUNCH();
     {
         LongRows L;
-        long_rows(ctx, ucount.p, nc, L);
-        if (L.nch) {
+        long_rows(ctx, ucount.p, nc, m, L);
+        if (L.grid) {
             LaunchTimer lt(ctx);
-            k_compact_long<<<(int)std::min<int64_t>(L.nch, 16LL * ctx->sm_count), 256, 0,
-                             ctx->stream>>>(rstart.p, ucount.p, L.list.p, L.cb.p, L.n, L.nch, uk.p,
-                                            uw.p, key_to_pos, tail.p, w.p);
+            k_compact_long<<<L.grid, 256, 0, ctx->stream>>>(rstart.p, ucount.p, L.list.p, L.cb.p,
+                                                            L.cnt.p, uk.p, uw.p, key_to_pos, tail.p,
+                                                            w.p);
         }
         VG_CHECK_LAUNCH();
     }
-    vg_sync(ctx);
     return vg_graph_wrap(ctx, nc, m, ucount.detach(), tail.detach(), w.detach());
 }

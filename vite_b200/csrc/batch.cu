@@ -372,7 +372,7 @@ void compose_levels(vg_batch *b, const std::vector<size_t> &which) {
     VG_CHECK_LAUNCH();
     { LaunchTimer lt(ctx); k_mark_used<<<grid, 256, 0, ctx->stream>>>(cvr.p, n, used.p); }
     VG_CHECK_LAUNCH();
-    vg_exclusive_scan_i32_to_i64(ctx, used.p, rank.p, n);
+    vg_scan_i32_async(ctx, used.p, rank.p, n, nullptr);
     std::vector<ComposeJob> cj;
     std::vector<int64_t> cb(1, 0);
     for (size_t k : which) {

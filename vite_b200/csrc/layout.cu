@@ -237,8 +237,6 @@ bool vg_local_structure(vg_ctx *ctx, const vg_graph *g) {
     return h[1] > 0 && (double)h[0] >= 0.1 * (double)h[1];
 }
 
-int64_t vg_exclusive_scan_i64(vg_ctx *ctx, int64_t *data, int64_t n);
-
 // graph with rows in `from` order; tails renamed through `rename`
 static vg_graph *move_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *from,
                            const int32_t *rename) {
@@ -250,7 +248,7 @@ static vg_graph *move_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *from,
         k_gather_deg<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(g->rowptr, from, nv, rp.p);
     }
     VG_CHECK_LAUNCH();
-    vg_exclusive_scan_i64(ctx, rp.p, nv + 1);
+    vg_scan_i64_async(ctx, rp.p, nv + 1, nullptr);
     DevBuf<int32_t> tail(ctx, ne);
     DevBuf<double> w(ctx, ne);
     if (nv) {

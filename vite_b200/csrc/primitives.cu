@@ -9,10 +9,14 @@ namespace {
 constexpr int SCAN_BLOCK = 256;
 constexpr int SCAN_ITEMS = 8;
 constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
+constexpr int SCAN_ONE = 1024;                     // threads of the single-CTA scan
+constexpr int64_t SCAN_ONE_MAX = 4LL * SCAN_ONE * SCAN_ITEMS; // single-CTA below this
 
-// exclusive block scan of one int64 per thread; returns the block total in *total
+// exclusive block scan of one int64 per thread; returns the block total in *total.
+// Ends with a barrier, so a block may call it again in a loop.
+template <int NT>
 __device__ int64_t block_exclusive_scan(int64_t v, int64_t *total) {
-    __shared__ int64_t warp_sums[SCAN_BLOCK / 32];
+    __shared__ int64_t warp_sums[NT / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int64_t x = v;
 #pragma unroll
@@ -23,23 +27,25 @@ __device__ int64_t block_exclusive_scan(int64_t v, int64_t *total) {
     if (lane == 31) warp_sums[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        int64_t s = lane < SCAN_BLOCK / 32 ? warp_sums[lane] : 0;
+        int64_t s = lane < NT / 32 ? warp_sums[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             int64_t y = __shfl_up_sync(0xffffffffu, s, o);
             if (lane >= o) s += y;
         }
-        if (lane < SCAN_BLOCK / 32) warp_sums[lane] = s;
+        if (lane < NT / 32) warp_sums[lane] = s;
     }
     __syncthreads();
     const int64_t warp_prefix = warp ? warp_sums[warp - 1] : 0;
-    *total = warp_sums[SCAN_BLOCK / 32 - 1];
+    *total = warp_sums[NT / 32 - 1];
     __syncthreads();
     return warp_prefix + x - v;
 }
 
+// per-tile sums: part[t] = sum of tile t
 template <class TIn>
-__global__ void k_scan_reduce(const TIn *__restrict__ in, int64_t n, int64_t *__restrict__ part) {
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_reduce(const TIn *__restrict__ in, int64_t n,
+                                                            int64_t *__restrict__ part) {
     const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
     int64_t s = 0;
 #pragma unroll
@@ -48,13 +54,42 @@ __global__ void k_scan_reduce(const TIn *__restrict__ in, int64_t n, int64_t *__
         if (i < n) s += (int64_t)in[i];
     }
     int64_t total;
-    block_exclusive_scan(s, &total);
+    block_exclusive_scan<SCAN_BLOCK>(s, &total);
     if (threadIdx.x == 0) part[blockIdx.x] = total;
 }
 
+// One CTA scans all n elements in chunks of SCAN_ONE * SCAN_ITEMS, carrying the
+// running sum; *total (when not null) gets the sum of all n. in may equal out:
+// every thread reads its items before it writes them and owns them alone.
 template <class TIn>
-__global__ void k_scan_down(const TIn *__restrict__ in, int64_t *__restrict__ out, int64_t n,
-                            const int64_t *__restrict__ part) {
+__global__ void __launch_bounds__(SCAN_ONE) k_scan_one(const TIn *in, int64_t *out, int64_t n,
+                                                      int64_t *total) {
+    int64_t carry = 0;
+    for (int64_t base = 0; base < n; base += (int64_t)SCAN_ONE * SCAN_ITEMS) {
+        const int64_t b = base + (int64_t)threadIdx.x * SCAN_ITEMS;
+        int64_t v[SCAN_ITEMS];
+        int64_t s = 0;
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; k++) {
+            v[k] = b + k < n ? (int64_t)in[b + k] : 0;
+            s += v[k];
+        }
+        int64_t tot;
+        int64_t run = block_exclusive_scan<SCAN_ONE>(s, &tot) + carry;
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; k++) {
+            if (b + k < n) out[b + k] = run;
+            run += v[k];
+        }
+        carry += tot;
+    }
+    if (total && threadIdx.x == 0) *total = carry;
+}
+
+// down sweep of tile t from its exclusive prefix part[t]; in may equal out (as above)
+template <class TIn>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_down(const TIn *in, int64_t *out, int64_t n,
+                                                          const int64_t *__restrict__ part) {
     const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
     int64_t v[SCAN_ITEMS];
     int64_t s = 0;
@@ -65,7 +100,7 @@ __global__ void k_scan_down(const TIn *__restrict__ in, int64_t *__restrict__ ou
         s += v[k];
     }
     int64_t total;
-    int64_t run = block_exclusive_scan(s, &total) + (part ? part[blockIdx.x] : 0);
+    int64_t run = block_exclusive_scan<SCAN_BLOCK>(s, &total) + part[blockIdx.x];
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; k++) {
         const int64_t i = base + k;
@@ -74,77 +109,64 @@ __global__ void k_scan_down(const TIn *__restrict__ in, int64_t *__restrict__ ou
     }
 }
 
+// Small inputs: one launch. Larger: tile sums, one CTA scans them (and writes the
+// total), then the down sweep: three launches, no host round trip.
 template <class TIn>
-int64_t scan_impl(vg_ctx *ctx, const TIn *in, int64_t *out, int64_t n) {
-    if (n <= 0) return 0;
+void scan_async(vg_ctx *ctx, const TIn *in, int64_t *out, int64_t n, int64_t *dev_total) {
+    if (n <= SCAN_ONE_MAX) {
+        LaunchTimer lt(ctx);
+        k_scan_one<TIn><<<1, SCAN_ONE, 0, ctx->stream>>>(in, out, n, dev_total);
+        VG_CHECK_LAUNCH();
+        return;
+    }
     const int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
-    DevBuf<int64_t> part(ctx, tiles + 1);
+    DevBuf<int64_t> part(ctx, tiles);
     {
         LaunchTimer lt(ctx);
         k_scan_reduce<TIn><<<(unsigned)tiles, SCAN_BLOCK, 0, ctx->stream>>>(in, n, part.p);
     }
     VG_CHECK_LAUNCH();
-    // scan the tile totals (recursively when there are many tiles); part[tiles] = total
-    VG_CUDA(cudaMemsetAsync(part.p + tiles, 0, sizeof(int64_t), ctx->stream));
-    if (tiles > 1) {
-        const int64_t tot = vg_exclusive_scan_i64(ctx, part.p, tiles);
-        (void)tot;
-    } else {
-        // single tile: its exclusive prefix is 0
-        int64_t t0;
-        int64_t *h = (int64_t *)vg_pinned(ctx, sizeof(int64_t));
-        VG_CUDA(cudaMemcpyAsync(h, part.p, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-        vg_sync(ctx);
-        t0 = *h;
-        VG_CUDA(cudaMemsetAsync(part.p, 0, sizeof(int64_t), ctx->stream));
-        {
-            LaunchTimer lt(ctx);
-            k_scan_down<TIn><<<1, SCAN_BLOCK, 0, ctx->stream>>>(in, out, n, part.p);
-        }
-        VG_CHECK_LAUNCH();
-        return t0;
+    {
+        LaunchTimer lt(ctx);
+        k_scan_one<int64_t><<<1, SCAN_ONE, 0, ctx->stream>>>(part.p, part.p, tiles, dev_total);
     }
-    // total = last exclusive prefix + last tile's sum: read both after the down sweep
+    VG_CHECK_LAUNCH();
     {
         LaunchTimer lt(ctx);
         k_scan_down<TIn><<<(unsigned)tiles, SCAN_BLOCK, 0, ctx->stream>>>(in, out, n, part.p);
     }
     VG_CHECK_LAUNCH();
-    int64_t *h = (int64_t *)vg_pinned(ctx, 2 * sizeof(int64_t));
-    VG_CUDA(cudaMemcpyAsync(h, out + (n - 1), sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-    vg_sync(ctx);
-    const int64_t last_prefix = h[0];
-    TIn last_in;
-    VG_CUDA(cudaMemcpyAsync(h, in + (n - 1), sizeof(TIn), cudaMemcpyDeviceToHost, ctx->stream));
-    vg_sync(ctx);
-    memcpy(&last_in, h, sizeof(TIn));
-    return last_prefix + (int64_t)last_in;
 }
 
-// in-place int64 scan needs a copy of the input for the down sweep
-__global__ void k_copy_i64(const int64_t *__restrict__ a, int64_t *__restrict__ b, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x)
-        b[i] = a[i];
+template <class TIn>
+int64_t scan_total(vg_ctx *ctx, const TIn *in, int64_t *out, int64_t n) {
+    if (n <= 0) return 0;
+    DevBuf<int64_t> tot(ctx, 1);
+    scan_async<TIn>(ctx, in, out, n, tot.p);
+    int64_t *h = (int64_t *)vg_pinned(ctx, sizeof(int64_t));
+    VG_CUDA(cudaMemcpyAsync(h, tot.p, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    vg_sync(ctx);
+    return *h;
 }
 
 } // namespace
 
 int64_t vg_exclusive_scan_i64(vg_ctx *ctx, int64_t *data, int64_t n) {
-    if (n <= 0) return 0;
-    DevBuf<int64_t> tmp(ctx, n);
-    {
-        LaunchTimer lt(ctx);
-        k_copy_i64<<<vg_grid(ctx, n, 256), 256, 0, ctx->stream>>>(data, tmp.p, n);
-    }
-    VG_CHECK_LAUNCH();
-    return scan_impl<int64_t>(ctx, tmp.p, data, n);
+    return scan_total<int64_t>(ctx, data, data, n);
 }
 
 int64_t vg_exclusive_scan_i32_to_i64(vg_ctx *ctx, const int32_t *in, int64_t *out, int64_t n) {
-    return scan_impl<int32_t>(ctx, in, out, n);
+    return scan_total<int32_t>(ctx, in, out, n);
 }
 
+void vg_scan_i64_async(vg_ctx *ctx, int64_t *data, int64_t n, int64_t *dev_total) {
+    if (n > 0) scan_async<int64_t>(ctx, data, data, n, dev_total);
+}
+
+void vg_scan_i32_async(vg_ctx *ctx, const int32_t *in, int64_t *out, int64_t n,
+                       int64_t *dev_total) {
+    if (n > 0) scan_async<int32_t>(ctx, in, out, n, dev_total);
+}
 // ---------------------------------------------------------------------------------
 // stable LSD radix sort, 8-bit digits
 
@@ -238,7 +260,7 @@ void vg_radix_sort_pairs(vg_ctx *ctx, uint64_t *keys, uint32_t *vals, int64_t n,
                                                                           ntiles);
         }
         VG_CHECK_LAUNCH();
-        vg_exclusive_scan_i32_to_i64(ctx, counts.p, offsets.p, 256 * ntiles);
+        vg_scan_i32_async(ctx, counts.p, offsets.p, 256 * ntiles, nullptr);
         {
             LaunchTimer lt(ctx);
             k_radix_scatter<<<(unsigned)ntiles, RS_BLOCK, 0, ctx->stream>>>(
@@ -407,6 +429,6 @@ vg_graph *vg_csr_from_triples(vg_ctx *ctx, int64_t nv, DevBuf<int32_t> &src, Dev
         VG_CHECK_LAUNCH();
     }
     w.release();
-    vg_exclusive_scan_i64(ctx, rowptr.p, nv + 1);
+    vg_scan_i64_async(ctx, rowptr.p, nv + 1, nullptr);
     return vg_graph_wrap(ctx, nv, u, rowptr.detach(), tail.detach(), weight.detach());
 }

@@ -164,7 +164,7 @@ vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm) {
                                                        flag_ref.p, flag_pos.p); }
         VG_CHECK_LAUNCH();
         nc = vg_exclusive_scan_i32_to_i64(ctx, flag_ref.p, rank_ref.p, nv);
-        vg_exclusive_scan_i32_to_i64(ctx, flag_pos.p, rank_pos.p, nv);
+        vg_scan_i32_async(ctx, flag_pos.p, rank_pos.p, nv, nullptr);
         { LaunchTimer lt(ctx);
           k_new_ids<<<grid, 256, 0, ctx->stream>>>(comm, nv, first_ref.p, rank_ref.p, first_pos.p,
                                                    rank_pos.p, new_ref.p, new_pos.p, next_ref.p,
@@ -571,7 +571,7 @@ extern "C" vg_status vg_generate_rgg(vg_ctx *ctx, int64_t n, double extra_percen
         { LaunchTimer lt(ctx); k_cells<<<grid, 256, 0, ctx->stream>>>(X.p, n, gr, cell.p, ccount.p); }
         VG_CHECK_LAUNCH();
         VG_CUDA(cudaMemsetAsync(cstart.p + ncell, 0, sizeof(int64_t), ctx->stream));
-        vg_exclusive_scan_i32_to_i64(ctx, ccount.p, cstart.p, ncell);
+        vg_scan_i32_async(ctx, ccount.p, cstart.p, ncell, nullptr);
         {
             // cstart[ncell] = n
             VG_CUDA(cudaMemcpyAsync(cstart.p + ncell, &n, sizeof(int64_t), cudaMemcpyHostToDevice,

@@ -165,9 +165,14 @@ vg_graph *vg_graph_wrap(vg_ctx *ctx, int64_t nv, int64_t ne, int64_t *rowptr, in
 // ---------------------------------------------------------------------------------
 // primitives (primitives.cu)
 
-// exclusive scan in place over n elements; returns the total
+// exclusive scan in place over n elements; returns the total (one stream sync)
 int64_t vg_exclusive_scan_i64(vg_ctx *ctx, int64_t *data, int64_t n);
 int64_t vg_exclusive_scan_i32_to_i64(vg_ctx *ctx, const int32_t *in, int64_t *out, int64_t n);
+// the same, stream-ordered with no host round trip; the total goes to *dev_total
+// (device memory) when dev_total is not null
+void vg_scan_i64_async(vg_ctx *ctx, int64_t *data, int64_t n, int64_t *dev_total);
+void vg_scan_i32_async(vg_ctx *ctx, const int32_t *in, int64_t *out, int64_t n,
+                       int64_t *dev_total);
 // stable LSD radix sort of 64-bit keys with 32-bit payloads over the low `bits` bits
 void vg_radix_sort_pairs(vg_ctx *ctx, uint64_t *keys, uint32_t *vals, int64_t n, int bits);
 // sum of a double array (deterministic)
