@@ -449,54 +449,63 @@ __global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
         for (int s = lane; s < cap; s += 32) keys[s] = EMPTY;
         __syncwarp();
         double selfLoop = 0.0;
-        for (int off = 0; off < d; off += 32) {
-            const int k = off + lane;
-            const bool has = k < d;
-            int32_t t = -1, c = -1;
-            double w = 0.0;
-            if (has) {
-                t = a.tail[e0 + k];
-                w = a.weight[e0 + k];
-                c = a.curr[t];
+        // groups of four 32-edge chunks: the group's tails and weights are loaded
+        // together, then their communities, so a group costs two round trips
+        for (int g0 = 0; g0 < d; g0 += 4 * 32) {
+            int32_t tt[4], cg[4];
+            double ww[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int k = g0 + j * 32 + lane;
+                tt[j] = k < d ? a.tail[e0 + k] : -1;
+                ww[j] = k < d ? a.weight[e0 + k] : 0.0;
             }
-            stage[lane] = w;
-            const unsigned peers = __match_any_sync(full, has ? c : (-1 - lane));
-            __syncwarp();
-            if (has && lane == __ffs(peers) - 1) {
-                uint32_t h = slot_hash(c, logcap);
-                bool fresh = false;
-                for (;;) {
-                    const int32_t kk = keys[h];
-                    if (kk == c) break;
-                    if (kk == EMPTY) {
-                        const int32_t old = atomicCAS(&keys[h], EMPTY, c);
-                        if (old == EMPTY) {
-                            fresh = true;
-                            break;
+#pragma unroll
+            for (int j = 0; j < 4; j++) cg[j] = tt[j] >= 0 ? a.curr[tt[j]] : -1;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (g0 + j * 32 >= d) break; // warp-uniform
+                const bool has = tt[j] >= 0;
+                const int32_t t = tt[j], c = cg[j];
+                stage[lane] = ww[j];
+                const unsigned peers = __match_any_sync(full, has ? c : (-1 - lane));
+                __syncwarp();
+                if (has && lane == __ffs(peers) - 1) {
+                    uint32_t h = slot_hash(c, logcap);
+                    bool fresh = false;
+                    for (;;) {
+                        const int32_t kk = keys[h];
+                        if (kk == c) break;
+                        if (kk == EMPTY) {
+                            const int32_t old = atomicCAS(&keys[h], EMPTY, c);
+                            if (old == EMPTY) {
+                                fresh = true;
+                                break;
+                            }
+                            if (old == c) break;
                         }
-                        if (old == c) break;
+                        h = (h + 1) & (cap - 1);
                     }
-                    h = (h + 1) & (cap - 1);
+                    unsigned m = peers & (peers - 1);
+                    double acc = fresh ? stage[lane] : __dadd_rn(vals[h], stage[lane]);
+                    while (m) {
+                        const int b = __ffs(m) - 1;
+                        acc = __dadd_rn(acc, stage[b]);
+                        m &= m - 1;
+                    }
+                    vals[h] = acc;
                 }
-                unsigned m = peers & (peers - 1);
-                double acc = fresh ? stage[lane] : __dadd_rn(vals[h], stage[lane]);
-                while (m) {
-                    const int b = __ffs(m) - 1;
-                    acc = __dadd_rn(acc, stage[b]);
-                    m &= m - 1;
+                const unsigned selfm = __ballot_sync(full, has && t == v);
+                {
+                    unsigned m = selfm;
+                    while (m) {
+                        const int b = __ffs(m) - 1;
+                        selfLoop = __dadd_rn(selfLoop, stage[b]);
+                        m &= m - 1;
+                    }
                 }
-                vals[h] = acc;
+                __syncwarp();
             }
-            const unsigned selfm = __ballot_sync(full, has && t == v);
-            {
-                unsigned m = selfm;
-                while (m) {
-                    const int b = __ffs(m) - 1;
-                    selfLoop = __dadd_rn(selfLoop, stage[b]);
-                    m &= m - 1;
-                }
-            }
-            __syncwarp();
         }
         // counter[0]: the current community's entry, if any neighbour is in it
         double counter0 = 0.0;
@@ -512,6 +521,23 @@ __global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
                 h = (h + 1) & (cap - 1);
             }
         }
+        // the other communities, compacted to the front of the table: a kept slot
+        // moves to the count of kept slots before it, never past a slot not yet read
+        int nk = 0;
+        for (int base = 0; base < cap; base += 32) {
+            const int32_t kk = keys[base + lane];
+            const double vv = vals[base + lane];
+            const bool keep = kk != EMPTY && kk != cc;
+            const unsigned bm = __ballot_sync(full, keep);
+            __syncwarp();
+            if (keep) {
+                const int dst = nk + __popc(bm & ((1u << lane) - 1u));
+                keys[dst] = kk;
+                vals[dst] = vv;
+            }
+            nk += __popc(bm);
+            __syncwarp();
+        }
         const double vd = a.vdeg[v];
         double ccDeg;
         int32_t ccSize;
@@ -521,18 +547,32 @@ __global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
         double gain = 0.0;
         int32_t cand = INT_MAX, csz = 0;
         bool ok = false;
-        for (int s = lane; s < cap; s += 32) {
-            const int32_t kk = keys[s];
-            if (kk == EMPTY || kk == cc) continue;
-            double ay;
-            int32_t sz;
-            load_comm(a, kk, ay, sz);
-            const double g = gain_of(vals[s], eix, vd, ay, ax, cst);
-            if (g > 0.0 && better(true, g, kk, ok, gain, cand, a.ref)) {
-                gain = g;
-                cand = kk;
-                csz = sz;
-                ok = true;
+        // four candidates per lane per round, their community loads issued together;
+        // the (gain, id) order makes the winner independent of the visiting order
+        for (int i0 = 0; i0 < nk; i0 += 4 * 32) {
+            int32_t kq[4], sq[4];
+            double aq[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int i = i0 + j * 32 + lane;
+                kq[j] = i < nk ? keys[i] : EMPTY;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                aq[j] = 0.0;
+                sq[j] = 0;
+                if (kq[j] != EMPTY) load_comm(a, kq[j], aq[j], sq[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (kq[j] == EMPTY) continue;
+                const double g = gain_of(vals[i0 + j * 32 + lane], eix, vd, aq[j], ax, cst);
+                if (g > 0.0 && better(true, g, kq[j], ok, gain, cand, a.ref)) {
+                    gain = g;
+                    cand = kq[j];
+                    csz = sq[j];
+                    ok = true;
+                }
             }
         }
 #pragma unroll
@@ -681,18 +721,60 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
         double gain = 0.0;
         int32_t cand = INT_MAX, csz = 0;
         bool ok = false;
-        for (int64_t s = threadIdx.x; s < cap; s += CT_THREADS) {
-            const int32_t kk = keys[s];
-            if (kk == EMPTY || kk == cc) continue;
-            double ay;
-            int32_t sz;
-            load_comm(a, kk, ay, sz);
-            const double g = gain_of(vals[s], eix, vd, ay, ax, cst);
-            if (g > 0.0 && better(true, g, kk, ok, gain, cand, a.ref)) {
-                gain = g;
-                cand = kk;
-                csz = sz;
-                ok = true;
+        // the other communities, compacted to the front of the table in slot order:
+        // a kept slot moves to the count of kept slots before it, so no write lands
+        // on a slot not yet read (each group's reads end at the barrier before its
+        // writes)
+        int64_t nk = 0;
+        for (int64_t base = 0; base < cap; base += CT_THREADS) {
+            const int64_t s = base + threadIdx.x;
+            const int32_t kk = s < cap ? keys[s] : EMPTY;
+            const double vv = s < cap ? vals[s] : 0.0;
+            const bool keep = kk != EMPTY && kk != cc;
+            const unsigned bm = __ballot_sync(full, keep);
+            if (lane == 0) sh.red_c[warp] = __popc(bm);
+            __syncthreads();
+            int before = 0, tot = 0;
+#pragma unroll
+            for (int w = 0; w < CT_THREADS / 32; w++) {
+                const int c = sh.red_c[w];
+                before += w < warp ? c : 0;
+                tot += c;
+            }
+            if (keep) {
+                const int64_t dst = nk + before + __popc(bm & ((1u << lane) - 1u));
+                keys[dst] = kk;
+                vals[dst] = vv;
+            }
+            nk += tot;
+            __syncthreads();
+        }
+        // four candidates per thread per round, their community loads issued together
+        for (int64_t i0 = 0; i0 < nk; i0 += 4 * CT_THREADS) {
+            int32_t kq[4], sq[4];
+            double aq[4], vq[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int64_t i = i0 + j * CT_THREADS + threadIdx.x;
+                kq[j] = i < nk ? keys[i] : EMPTY;
+                vq[j] = i < nk ? vals[i] : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                aq[j] = 0.0;
+                sq[j] = 0;
+                if (kq[j] != EMPTY) load_comm(a, kq[j], aq[j], sq[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (kq[j] == EMPTY) continue;
+                const double g = gain_of(vq[j], eix, vd, aq[j], ax, cst);
+                if (g > 0.0 && better(true, g, kq[j], ok, gain, cand, a.ref)) {
+                    gain = g;
+                    cand = kq[j];
+                    csz = sq[j];
+                    ok = true;
+                }
             }
         }
 #pragma unroll
