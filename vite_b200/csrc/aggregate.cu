@@ -33,12 +33,16 @@ __global__ void k_vertex_keys(int64_t nv, const int32_t *__restrict__ pos,
     }
 }
 
+// k-th vertex in grouped order: its degree, and where its row starts in the CSR
 __global__ void k_sorted_deg(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ pos,
-                             const uint32_t *__restrict__ order, int64_t nv, int64_t *__restrict__ deg) {
+                             const uint32_t *__restrict__ order, int64_t nv, int64_t *__restrict__ deg,
+                             int64_t *__restrict__ src_start) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nv;
          k += (int64_t)gridDim.x * blockDim.x) {
         const int32_t p = pos_of(pos, order[k]);
-        deg[k] = rowptr[p + 1] - rowptr[p];
+        const int64_t e0 = rowptr[p];
+        deg[k] = rowptr[p + 1] - e0;
+        src_start[k] = e0;
     }
 }
 
@@ -57,9 +61,8 @@ constexpr int64_t COPY_CHUNK = 4096;
 
 // vertices in grouped order: each one's row goes to its segment, neighbours renamed
 // to their ordering keys
-__global__ void k_group_copy(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
-                             const double *__restrict__ w, const int32_t *__restrict__ pos,
-                             const uint32_t *__restrict__ order, const int64_t *__restrict__ off,
+__global__ void k_group_copy(const int32_t *__restrict__ tail, const double *__restrict__ w,
+                             const int64_t *__restrict__ src_start, const int64_t *__restrict__ off,
                              int64_t nv, const int32_t *__restrict__ new_key,
                              int32_t *__restrict__ gk, double *__restrict__ gw) {
     const int sub = threadIdx.x & 7;
@@ -68,11 +71,22 @@ __global__ void k_group_copy(const int64_t *__restrict__ rowptr, const int32_t *
     for (int64_t k = grp; k < nv; k += ng) {
         const int64_t o = off[k], len = off[k + 1] - o;
         if (len > LONG_ROW) continue;
-        const int32_t p = pos_of(pos, order[k]);
-        const int64_t e0 = rowptr[p];
-        for (int64_t j = sub; j < len; j += 8) {
-            gk[o + j] = new_key[tail[e0 + j]];
-            gw[o + j] = w[e0 + j];
+        const int64_t e0 = src_start[k];
+        // two entries per lane per step: both tails are loaded before the key gathers
+        for (int64_t j = sub; j < len; j += 16) {
+            const bool two = j + 8 < len;
+            const int32_t t0 = tail[e0 + j];
+            const int32_t t1 = two ? tail[e0 + j + 8] : 0;
+            const double w0 = w[e0 + j];
+            const double w1 = two ? w[e0 + j + 8] : 0.0;
+            const int32_t k0 = new_key[t0];
+            const int32_t k1 = two ? new_key[t1] : 0;
+            gk[o + j] = k0;
+            gw[o + j] = w0;
+            if (two) {
+                gk[o + j + 8] = k1;
+                gw[o + j + 8] = w1;
+            }
         }
     }
 }
@@ -106,9 +120,8 @@ __device__ __forceinline__ int64_t chunk_owner(const int64_t *__restrict__ cb, i
     return lo;
 }
 
-__global__ void k_group_copy_long(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
-                                  const double *__restrict__ w, const int32_t *__restrict__ pos,
-                                  const uint32_t *__restrict__ order, const int64_t *__restrict__ off,
+__global__ void k_group_copy_long(const int32_t *__restrict__ tail, const double *__restrict__ w,
+                                  const int64_t *__restrict__ src_start, const int64_t *__restrict__ off,
                                   const int32_t *__restrict__ list, const int64_t *__restrict__ cb,
                                   const int64_t *__restrict__ cnt, const int32_t *__restrict__ new_key,
                                   int32_t *__restrict__ gk, double *__restrict__ gw) {
@@ -117,7 +130,7 @@ __global__ void k_group_copy_long(const int64_t *__restrict__ rowptr, const int3
         const int64_t q = chunk_owner(cb, nl, c);
         const int64_t k = list[q];
         const int64_t o = off[k], len = off[k + 1] - o;
-        const int64_t e0 = rowptr[pos_of(pos, order[k])];
+        const int64_t e0 = src_start[k];
         const int64_t j0 = (c - cb[q]) * COPY_CHUNK, j1 = min(j0 + COPY_CHUNK, len);
         for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
             gk[o + j] = new_key[tail[e0 + j]];
@@ -163,8 +176,9 @@ struct HashWarpSmem {
     int32_t keys[H_CAP];
     double vals[H_CAP];
     uint64_t list[H_MAXU + 32]; // (key << 32 | slot) of the distinct keys
-    double stage[32];
+    alignas(16) double stage[32];
 };
+
 
 __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
     int64_t nc, const int64_t *__restrict__ rstart, const int32_t *__restrict__ gk,
@@ -186,52 +200,60 @@ __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
         __syncwarp();
         int U = 0;
         bool over = false;
-        for (int64_t base = 0; base < L; base += 32) {
-            const int64_t i = base + lane;
-            const bool has = i < L;
-            int32_t k = -2 - lane; // distinct non-keys for idle lanes
-            double w = 0.0;
-            if (has) {
-                k = gk[b + i];
-                w = gw[b + i];
+        // groups of four 32-entry chunks, the group's loads issued together
+        for (int64_t base = 0; base < L && !over; base += 4 * 32) {
+            int32_t kq[4];
+            double wq[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int64_t i = base + j * 32 + lane;
+                kq[j] = -2 - lane; // distinct non-keys for idle lanes
+                wq[j] = 0.0;
+                if (i < L) {
+                    kq[j] = gk[b + i];
+                    wq[j] = gw[b + i];
+                }
             }
-            S.stage[lane] = w;
-            const unsigned peers = __match_any_sync(full, k);
-            __syncwarp();
-            bool fresh = false;
-            int slot = 0;
-            if (has && lane == __ffs(peers) - 1) {
-                uint32_t h = ((uint32_t)k * 2654435761u) >> (32 - logcap);
-                for (;;) {
-                    const int32_t kk = S.keys[h];
-                    if (kk == k) break;
-                    if (kk == H_EMPTY) {
-                        const int32_t old = atomicCAS(&S.keys[h], H_EMPTY, k);
-                        if (old == H_EMPTY) {
-                            fresh = true;
-                            break;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (base + j * 32 >= L) break; // warp-uniform
+                const bool has = base + j * 32 + lane < L;
+                const int32_t k = kq[j];
+                const double w = wq[j];
+                S.stage[lane] = w;
+                const unsigned peers = __match_any_sync(full, k);
+                __syncwarp();
+                bool fresh = false;
+                int slot = 0;
+                if (has && lane == __ffs(peers) - 1) {
+                    uint32_t h = ((uint32_t)k * 2654435761u) >> (32 - logcap);
+                    for (;;) {
+                        const int32_t kk = S.keys[h];
+                        if (kk == k) break;
+                        if (kk == H_EMPTY) {
+                            const int32_t old = atomicCAS(&S.keys[h], H_EMPTY, k);
+                            if (old == H_EMPTY) {
+                                fresh = true;
+                                break;
+                            }
+                            if (old == k) break;
                         }
-                        if (old == k) break;
+                        h = (h + 1) & (uint32_t)(cap - 1);
                     }
-                    h = (h + 1) & (uint32_t)(cap - 1);
+                    slot = (int)h;
+                    double acc = fresh ? w : __dadd_rn(S.vals[h], w);
+                    const unsigned above = peers & ~((2u << lane) - 1u);
+                    if (above) acc = vg_fold_above(acc, S.stage, above);
+                    S.vals[h] = acc;
                 }
-                slot = (int)h;
-                double acc = fresh ? w : __dadd_rn(S.vals[h], w);
-                unsigned m = peers & (peers - 1);
-                while (m) {
-                    const int q = __ffs(m) - 1;
-                    acc = __dadd_rn(acc, S.stage[q]);
-                    m &= m - 1;
+                const unsigned fm = __ballot_sync(full, fresh);
+                if (fresh) S.list[U + __popc(fm & lt)] = ((uint64_t)(uint32_t)k << 32) | (uint32_t)slot;
+                U += __popc(fm);
+                __syncwarp();
+                if (U > H_MAXU) { // too many distinct keys for the table: the sorted path
+                    over = true;
+                    break;
                 }
-                S.vals[h] = acc;
-            }
-            const unsigned fm = __ballot_sync(full, fresh);
-            if (fresh) S.list[U + __popc(fm & lt)] = ((uint64_t)(uint32_t)k << 32) | (uint32_t)slot;
-            U += __popc(fm);
-            __syncwarp();
-            if (U > H_MAXU) { // too many distinct keys for the table: the sorted path
-                over = true;
-                break;
             }
         }
         if (over) {
@@ -489,11 +511,12 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
         vg_radix_sort_pairs(ctx, vkeys.p, vorder.p, nv, kbits);
     }
     // 2. segment offsets
-    DevBuf<int64_t> off(ctx, nv + 1), rstart(ctx, nc + 1);
+    DevBuf<int64_t> off(ctx, nv + 1), rstart(ctx, nc + 1), src_start(ctx, nv);
     VG_CUDA(cudaMemsetAsync(off.p + nv, 0, sizeof(int64_t), ctx->stream));
     if (nv) {
         { LaunchTimer lt(ctx);
-          k_sorted_deg<<<grid, 256, 0, ctx->stream>>>(g->rowptr, pos, vorder.p, nv, off.p); }
+          k_sorted_deg<<<grid, 256, 0, ctx->stream>>>(g->rowptr, pos, vorder.p, nv, off.p,
+                                                      src_start.p); }
         VG_CHECK_LAUNCH();
     }
     vg_scan_i64_async(ctx, off.p, nv + 1, nullptr);
@@ -510,7 +533,7 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     if (ne) {
         LaunchTimer lt(ctx);
         k_group_copy<<<vg_grid(ctx, nv * 8, 256), 256, 0, ctx->stream>>>(
-            g->rowptr, g->tail, g->weight, pos, vorder.p, off.p, nv, new_key, gk.p, gw.p);
+            g->tail, g->weight, src_start.p, off.p, nv, new_key, gk.p, gw.p);
     }
     VG_CHECK_LAUNCH();
     {
@@ -518,14 +541,15 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
         long_rows(ctx, off.p, nv, ne, L);
         if (L.grid) {
             LaunchTimer lt(ctx);
-            k_group_copy_long<<<L.grid, 256, 0, ctx->stream>>>(g->rowptr, g->tail, g->weight, pos,
-                                                               vorder.p, off.p, L.list.p, L.cb.p,
-                                                               L.cnt.p, new_key, gk.p, gw.p);
+            k_group_copy_long<<<L.grid, 256, 0, ctx->stream>>>(g->tail, g->weight, src_start.p,
+                                                               off.p, L.list.p, L.cb.p, L.cnt.p,
+                                                               new_key, gk.p, gw.p);
         }
         VG_CHECK_LAUNCH();
     }
     vorder.release();
     off.release();
+    src_start.release();
     // 4. sort + fold per segment
     DevBuf<int32_t> uk(ctx, ne);
     DevBuf<double> uw(ctx, ne);

@@ -486,13 +486,9 @@ __global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
                         }
                         h = (h + 1) & (cap - 1);
                     }
-                    unsigned m = peers & (peers - 1);
+                    const unsigned above = peers & ~((2u << lane) - 1u);
                     double acc = fresh ? stage[lane] : __dadd_rn(vals[h], stage[lane]);
-                    while (m) {
-                        const int b = __ffs(m) - 1;
-                        acc = __dadd_rn(acc, stage[b]);
-                        m &= m - 1;
-                    }
+                    if (above) acc = vg_fold_above(acc, stage, above);
                     vals[h] = acc;
                 }
                 const unsigned selfm = __ballot_sync(full, has && t == v);
@@ -614,7 +610,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
                                                           double *__restrict__ gvals, int64_t gcap) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ CtaShared sh;
-    __shared__ double stage[CT_THREADS];
+    __shared__ __align__(16) double stage[CT_THREADS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
     double *vals;
@@ -661,12 +657,8 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
             __syncwarp();
             if (has && lane == __ffs(peers) - 1) {
                 double acc = stage[threadIdx.x];
-                unsigned m = peers & (peers - 1);
-                while (m) {
-                    const int b = __ffs(m) - 1;
-                    acc = __dadd_rn(acc, stage[(threadIdx.x & ~31) + b]);
-                    m &= m - 1;
-                }
+                const unsigned above = peers & ~((2u << lane) - 1u);
+                if (above) acc = vg_fold_above(acc, stage + (threadIdx.x & ~31), above);
                 uint32_t h = slot_hash(c, logcap);
                 for (;;) {
                     const int32_t kk = keys[h];

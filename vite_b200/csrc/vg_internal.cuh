@@ -193,6 +193,22 @@ int vg_grid(vg_ctx *ctx, int64_t work, int block, int per_sm = 8);
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31; }
 
+// A chunk leader's left fold: acc + stage[j] for each lane j of `above` (its peers
+// above it) in lane order; stage holds the warp's 32 values, 16-byte aligned. Every
+// read is issued before the first add, so the chain waits on the additions only.
+__device__ __forceinline__ double vg_fold_above(double acc, const double *stage, unsigned above) {
+    const double2 *s2 = reinterpret_cast<const double2 *>(stage);
+    double2 x[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) x[j] = s2[j];
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if (above & (1u << (2 * j))) acc = __dadd_rn(acc, x[j].x);
+        if (above & (2u << (2 * j))) acc = __dadd_rn(acc, x[j].y);
+    }
+    return acc;
+}
+
 // counter-based generator shared with the oracle's restatement
 __host__ __device__ __forceinline__ uint64_t vg_sm64(uint64_t x) {
     x += 0x9E3779B97F4A7C15ULL;
