@@ -20,12 +20,15 @@
 
 namespace {
 
-constexpr int NCLS = 5;
-// class by degree: 0: <= TMAX (one thread per vertex) 1: <= 32 (one warp, one chunk)
-// 2: <= WT_MAXDEG (warp, shared-memory table) 3: <= CT_MAXDEG (CTA, shared table)
-// 4: above (CTA, table in global scratch)
+constexpr int NCLS = 6;
+// class by degree: 0: <= TMAX (one thread per vertex) 1: <= 32 (one thread per vertex)
+// 2: <= WS_MAXDEG (warp, small shared-memory table) 3: <= WT_MAXDEG (warp, large
+// table) 4: <= CT_MAXDEG (CTA, shared table) 5: above (CTA, table in global scratch)
 constexpr int TMAX = 16;
 constexpr int TB = 256;
+#ifndef VG_WS_MAXDEG
+#define VG_WS_MAXDEG 128
+#endif
 #ifndef VG_WT_MAXDEG
 #define VG_WT_MAXDEG 512
 #endif
@@ -35,9 +38,16 @@ constexpr int TB = 256;
 #ifndef VG_T32
 #define VG_T32 1
 #endif
+#ifndef VG_T32_MINB
+#define VG_T32_MINB 4 // resident CTAs per SM the degree-<=32 list kernel is sized for
+#endif
+constexpr int WS_MAXDEG = VG_WS_MAXDEG;
+constexpr int WS_CAP = 256;  // > 2 * WS_MAXDEG - 1: load factor at most one half
+constexpr int WS_WARPS = 8;
 constexpr int WT_MAXDEG = VG_WT_MAXDEG;
 constexpr int WT_CAP = 1024;
 constexpr int WT_WARPS = 4;
+static_assert(2 * WS_MAXDEG <= WS_CAP && 2 * WT_MAXDEG <= WT_CAP, "warp tables too small");
 constexpr int CT_MAXDEG = VG_CT_MAXDEG;
 constexpr int CT_CAP = 8192;
 constexpr int CT_THREADS = 256;
@@ -46,9 +56,10 @@ constexpr int32_t EMPTY = -1;
 __host__ __device__ __forceinline__ int degree_class(int64_t d) {
     if (d <= TMAX) return 0;
     if (VG_T32 && d <= 32) return 1;
-    if (d <= WT_MAXDEG) return 2;
-    if (d <= CT_MAXDEG) return 3;
-    return 4;
+    if (d <= WS_MAXDEG) return 2;
+    if (d <= WT_MAXDEG) return 3;
+    if (d <= CT_MAXDEG) return 4;
+    return 5;
 }
 
 // community update (localCupdate, Comm of graph.hpp:77-82) packed in 16 bytes so
@@ -146,8 +157,18 @@ __device__ __forceinline__ void commit_vertex(const SweepArgs &a, int32_t v, int
 // accumulated in an interleaved shared-memory slot of the community's first
 // occurrence. Candidate degrees are gathered eight at a time.
 
+// 8-byte global -> shared copy that bypasses the registers (completes at
+// cp_async_wait_all, visible to the issuing thread)
+__device__ __forceinline__ void cp_async8(double *dst_smem, const double *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 template <bool LIST, int T, int NT>
-__global__ void __launch_bounds__(NT, (T <= 16 ? 3 : 3)) k_sweep_thread(
+__global__ void __launch_bounds__(NT, (T <= 16 ? 3 : VG_T32_MINB)) k_sweep_thread(
     SweepArgs a, const int32_t *__restrict__ list, int64_t count) {
     __shared__ double ssum[T][NT];
     const int tid = threadIdx.x;
@@ -166,35 +187,46 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? 3 : 3)) k_sweep_thread(
         const double vd = a.vdeg[v];
         const double ccDeg = __ldg(a.cdeg + cc);
         int32_t c[T];
-        double selfLoop = 0.0;
-        uint32_t first = 0; // bit j: edge j is the first occurrence of its community
+        uint32_t selfm = 0; // bit j: edge j is a self loop
         {
-            double w[T];
+            // weights go straight to the thread's shared-memory slots (asynchronous
+            // copies); tails are loaded up front, then their communities gathered
+            int32_t t[T];
 #pragma unroll
             for (int j = 0; j < T; j++) {
-                c[j] = -1;
-                w[j] = 0.0;
+                t[j] = -1;
                 if (j < d) {
-                    const int32_t t = __ldcs(a.tail + e0 + j);
-                    w[j] = __ldcs(a.weight + e0 + j);
-                    c[j] = __ldg(a.curr + t);
-                    if (t == v) selfLoop = __dadd_rn(selfLoop, w[j]);
+                    t[j] = __ldcs(a.tail + e0 + j);
+                    cp_async8(&ssum[j][tid], a.weight + e0 + j);
                 }
             }
 #pragma unroll
             for (int j = 0; j < T; j++) {
+                c[j] = -1;
                 if (j < d) {
-                    int fj = j;
-#pragma unroll
-                    for (int k = j - 1; k >= 0; k--)
-                        if (c[k] == c[j]) fj = k;
-                    if (fj == j) {
-                        first |= 1u << j;
-                        ssum[j][tid] = w[j];
-                    } else {
-                        ssum[fj][tid] = __dadd_rn(ssum[fj][tid], w[j]);
-                    }
+                    c[j] = __ldg(a.curr + t[j]);
+                    if (t[j] == v) selfm |= 1u << j;
                 }
+            }
+        }
+        cp_async_wait_all();
+        double selfLoop = 0.0;
+#pragma unroll
+        for (int j = 0; j < T; j++)
+            if ((selfm >> j) & 1u) selfLoop = __dadd_rn(selfLoop, ssum[j][tid]);
+        // counters fold in place at the slot of each community's first occurrence,
+        // in CSR order (slot j still holds w_j when edge j is folded: only first
+        // occurrences receive additions)
+        uint32_t first = 0; // bit j: edge j is the first occurrence of its community
+#pragma unroll
+        for (int j = 0; j < T; j++) {
+            if (j < d) {
+                int fj = j;
+#pragma unroll
+                for (int k = j - 1; k >= 0; k--)
+                    if (c[k] == c[j]) fj = k;
+                if (fj == j) first |= 1u << j;
+                else ssum[fj][tid] = __dadd_rn(ssum[fj][tid], ssum[j][tid]);
             }
         }
         double counter0 = 0.0;
@@ -416,18 +448,23 @@ __device__ __forceinline__ uint32_t slot_hash(int32_t c, int logcap) {
 // weights in CSR order onto the table value, so each counter is the reference's
 // exact left fold.
 
-__global__ void __launch_bounds__(WT_WARPS * 32) k_sweep_warp(SweepArgs a,
-                                                               const int32_t *__restrict__ list,
-                                                               int64_t count) {
+// shared memory of a k_sweep_warp block: vals[WARPS][CAP], keys[WARPS][CAP], stage[WARPS][32]
+template <int CAP, int WARPS> constexpr size_t warp_smem_bytes() {
+    return (size_t)WARPS * CAP * (sizeof(double) + sizeof(int32_t)) + (size_t)WARPS * 32 * sizeof(double);
+}
+
+template <int CAP, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, CAP <= 256 ? 4 : 1) k_sweep_warp(
+    SweepArgs a, const int32_t *__restrict__ list, int64_t count) {
     extern __shared__ unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *vals = reinterpret_cast<double *>(smem_raw) + (size_t)warp * WT_CAP;
+    double *vals = reinterpret_cast<double *>(smem_raw) + (size_t)warp * CAP;
     int32_t *keys = reinterpret_cast<int32_t *>(reinterpret_cast<double *>(smem_raw) +
-                                                (size_t)WT_WARPS * WT_CAP) +
-                    (size_t)warp * WT_CAP;
+                                                (size_t)WARPS * CAP) +
+                    (size_t)warp * CAP;
     double *stage = reinterpret_cast<double *>(reinterpret_cast<int32_t *>(
-                        reinterpret_cast<double *>(smem_raw) + (size_t)WT_WARPS * WT_CAP) +
-                                               (size_t)WT_WARPS * WT_CAP) +
+                        reinterpret_cast<double *>(smem_raw) + (size_t)WARPS * CAP) +
+                                               (size_t)WARPS * CAP) +
                     (size_t)warp * 32;
     const unsigned full = 0xffffffffu;
     const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -1289,7 +1326,7 @@ struct Buckets {
     DevBuf<int32_t> list;
     std::vector<int64_t> start; // (numColor * NCLS) + 1 offsets
     int64_t ncolor = 1;
-    int64_t maxdeg_global = 0;  // largest degree in class 6
+    int64_t maxdeg_global = 0;  // largest degree of the global-table class
 };
 
 static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors, int64_t numColor,
@@ -1339,17 +1376,17 @@ static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors,
     vg_sync(ctx); // keep `fill` alive until the copy is done
 }
 
-static size_t warp_smem_bytes() {
-    return (size_t)WT_WARPS * WT_CAP * (sizeof(double) + sizeof(int32_t)) +
-           (size_t)WT_WARPS * 32 * sizeof(double);
-}
 static size_t cta_smem_bytes() { return (size_t)CT_CAP * (sizeof(double) + sizeof(int32_t)); }
 
 static void configure_kernels_once() {
     static bool done = false;
     if (done) return;
-    VG_CUDA(cudaFuncSetAttribute(k_sweep_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)warp_smem_bytes()));
+    VG_CUDA(cudaFuncSetAttribute(k_sweep_warp<WS_CAP, WS_WARPS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)warp_smem_bytes<WS_CAP, WS_WARPS>()));
+    VG_CUDA(cudaFuncSetAttribute(k_sweep_warp<WT_CAP, WT_WARPS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)warp_smem_bytes<WT_CAP, WT_WARPS>()));
     VG_CUDA(cudaFuncSetAttribute(k_sweep_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_smem_bytes()));
     done = true;
@@ -1388,10 +1425,16 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
             k_sweep_thread<true, 32, 128><<<vg_grid(ctx, n, 128, 12), 128, 0, ctx->stream>>>(a, list + s, n);
             break;
         case 2:
-            k_sweep_warp<<<vg_grid(ctx, n * 32, WT_WARPS * 32, 4), WT_WARPS * 32, warp_smem_bytes(),
-                           ctx->stream>>>(a, list + s, n);
+            k_sweep_warp<WS_CAP, WS_WARPS><<<vg_grid(ctx, n * 32, WS_WARPS * 32, 4), WS_WARPS * 32,
+                                             warp_smem_bytes<WS_CAP, WS_WARPS>(), ctx->stream>>>(
+                a, list + s, n);
             break;
         case 3:
+            k_sweep_warp<WT_CAP, WT_WARPS><<<vg_grid(ctx, n * 32, WT_WARPS * 32, 4), WT_WARPS * 32,
+                                             warp_smem_bytes<WT_CAP, WT_WARPS>(), ctx->stream>>>(
+                a, list + s, n);
+            break;
+        case 4:
             k_sweep_cta<false><<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, 2), CT_THREADS,
                                  cta_smem_bytes(), ctx->stream>>>(a, list + s, n, nullptr, nullptr, 0);
             break;
@@ -1470,7 +1513,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         while (cap < 2 * bk.maxdeg_global) cap <<= 1;
         int64_t n6 = 0;
         for (int64_t c = 0; c < numColor; c++)
-            n6 = std::max(n6, bk.start[c * NCLS + 5] - bk.start[c * NCLS + 4]);
+            n6 = std::max(n6, bk.start[c * NCLS + 6] - bk.start[c * NCLS + 5]);
         gt.blocks = (int)std::min<int64_t>(n6, (int64_t)ctx->sm_count * 2);
         gt.cap = cap;
         gt.keys.alloc(ctx, (size_t)cap * gt.blocks);
