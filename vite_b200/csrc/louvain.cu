@@ -150,22 +150,32 @@ __device__ __forceinline__ void commit_vertex(const SweepArgs &a, int32_t v, int
     }
 }
 
+// Global -> shared copies that bypass the registers: all of a thread's copies are
+// in flight together and complete at cp_async_wait_all (visible to the issuing
+// thread; a __syncwarp after the wait publishes them to the warp). The 16-byte
+// form needs 16-byte aligned addresses on both sides.
+__device__ __forceinline__ void cp_async4(void *dst_smem, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst_smem, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------------
 // classes 0 and 1: one thread per vertex (degree <= T). All edge loads are issued
 // up front (streaming hint on the CSR, read-only path on the gathered arrays);
 // each community's counter is the reference's left fold in CSR order,
 // accumulated in an interleaved shared-memory slot of the community's first
 // occurrence. Candidate degrees are gathered eight at a time.
-
-// 8-byte global -> shared copy that bypasses the registers (completes at
-// cp_async_wait_all, visible to the issuing thread)
-__device__ __forceinline__ void cp_async8(double *dst_smem, const double *src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
 
 template <bool LIST, int T, int NT>
 __global__ void __launch_bounds__(NT, (T <= 16 ? 3 : VG_T32_MINB)) k_sweep_thread(
@@ -367,8 +377,8 @@ constexpr int TILE_WARPS = VG_TILE_WARPS;
 template <int T>
 __global__ void __launch_bounds__(TILE_WARPS * 32, VG_TILE_MINB) k_sweep_tile(SweepArgs a, int64_t nv) {
     static_assert(32 * T <= TILE_CAP + 8, "the per-lane fallback layout must fit the buffer");
-    __shared__ int32_t st_all[TILE_WARPS][TILE_CAP + 8];
-    __shared__ double sw_all[TILE_WARPS][TILE_CAP + 8];
+    __shared__ __align__(16) int32_t st_all[TILE_WARPS][TILE_CAP + 8];
+    __shared__ __align__(16) double sw_all[TILE_WARPS][TILE_CAP + 8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int32_t *st = st_all[warp];
     double *sw = sw_all[warp];
@@ -394,28 +404,22 @@ __global__ void __launch_bounds__(TILE_WARPS * 32, VG_TILE_MINB) k_sweep_tile(Sw
         const int64_t A0 = E0 & ~3LL, B0 = E0 & ~1LL;
         int off_t, off_w; // where this lane's row starts in st / sw
         if (E1 - A0 <= TILE_CAP) {
-            // coalesced: int4 for tails, double2 for weights (16-byte aligned starts)
+            // coalesced 16-byte copies (16-byte aligned starts), all in flight at once
             const int64_t nt = (E1 - A0 + 3) >> 2, nw2 = (E1 - B0 + 1) >> 1;
             for (int64_t k = lane; k < nt; k += 32) {
                 const int64_t i = A0 + 4 * k;
                 if (i + 4 <= a.ne) {
-                    const int4 x = __ldcs(reinterpret_cast<const int4 *>(a.tail + i));
-                    st[4 * k] = x.x;
-                    st[4 * k + 1] = x.y;
-                    st[4 * k + 2] = x.z;
-                    st[4 * k + 3] = x.w;
+                    cp_async16(st + 4 * k, a.tail + i);
                 } else {
-                    for (int q = 0; q < 4 && i + q < a.ne; q++) st[4 * k + q] = __ldcs(a.tail + i + q);
+                    for (int q = 0; q < 4 && i + q < a.ne; q++) cp_async4(st + 4 * k + q, a.tail + i + q);
                 }
             }
             for (int64_t k = lane; k < nw2; k += 32) {
                 const int64_t i = B0 + 2 * k;
                 if (i + 2 <= a.ne) {
-                    const double2 x = __ldcs(reinterpret_cast<const double2 *>(a.weight + i));
-                    sw[2 * k] = x.x;
-                    sw[2 * k + 1] = x.y;
+                    cp_async16(sw + 2 * k, a.weight + i);
                 } else if (i < a.ne) {
-                    sw[2 * k] = __ldcs(a.weight + i);
+                    cp_async8(sw + 2 * k, a.weight + i);
                 }
             }
             off_t = (int)(e0 - A0);
@@ -424,13 +428,14 @@ __global__ void __launch_bounds__(TILE_WARPS * 32, VG_TILE_MINB) k_sweep_tile(Sw
             // long range (hub rows inside the tile): each lane copies its own short row
             if (live && d <= T) {
                 for (int j = 0; j < d; j++) {
-                    st[lane * T + j] = __ldcs(a.tail + e0 + j);
-                    sw[lane * T + j] = __ldcs(a.weight + e0 + j);
+                    cp_async4(st + lane * T + j, a.tail + e0 + j);
+                    cp_async8(sw + lane * T + j, a.weight + e0 + j);
                 }
             }
             off_t = lane * T;
             off_w = lane * T;
         }
+        cp_async_wait_all();
         __syncwarp();
         if (live && d <= T) tile_vertex<T>(a, v, d, cst, st + off_t, sw + off_w);
         __syncwarp();
