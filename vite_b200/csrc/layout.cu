@@ -37,9 +37,9 @@ __global__ void k_bfs_init(int64_t nv, uint64_t seed, int32_t *__restrict__ labe
 }
 
 // one level: vertices at distance step-1 claim their unlabeled neighbours. A warp
-// takes 32 consecutive vertices and walks the frontier rows among them one at a
-// time, lane j on entry j, so a row's claims are issued together instead of as a
-// chain of dependent loads and compare-and-swaps.
+// takes 32 consecutive vertices and walks the frontier rows among them four at a
+// time, eight lanes to a row, so a row's claims are issued together instead of as
+// a chain of dependent loads and compare-and-swaps.
 // unvisited vertices are found through the byte array of distances (255 =
 // unvisited), which stays in L2; the label's compare-and-swap settles races
 __device__ __forceinline__ unsigned long long bfs_claim(const int32_t *__restrict__ tail, int64_t e,
@@ -72,13 +72,18 @@ __global__ void k_bfs_step(const int64_t *__restrict__ rowptr, const int32_t *__
             e1 = rowptr[u + 1];
             lu = label[u];
         }
-        unsigned fm = __ballot_sync(full, front);
-        while (fm) {
-            const int src = __ffs(fm) - 1;
-            fm &= fm - 1;
+        // four groups of eight lanes: in round k, group g walks the row of the
+        // (4k + g)-th frontier vertex of the window (rounds are warp-uniform)
+        const unsigned fm = __ballot_sync(full, front);
+        const int nf = __popc(fm), grp = lane >> 3, sub = lane & 7;
+        for (int k = 0; 4 * k < nf; k++) {
+            const int r = 4 * k + grp;
+            const bool has = r < nf;
+            const int src = has ? (int)__fns(fm, 0, r + 1) : 0;
             const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
             const int32_t L = __shfl_sync(full, lu, src);
-            for (int64_t e = E0 + lane; e < E1; e += 32) mine += bfs_claim(tail, e, L, step, label, dist);
+            if (has)
+                for (int64_t e = E0 + sub; e < E1; e += 8) mine += bfs_claim(tail, e, L, step, label, dist);
         }
     }
 #pragma unroll
@@ -113,30 +118,44 @@ __global__ void k_inverse(const int32_t *__restrict__ perm, int64_t n, int32_t *
         inv[perm[k]] = (int32_t)k;
 }
 
+// k-th row of the moved graph: its degree and where it starts in the source CSR
 __global__ void k_gather_deg(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ from,
-                             int64_t n, int64_t *__restrict__ deg) {
+                             int64_t n, int64_t *__restrict__ deg, int64_t *__restrict__ src_start) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
          k += (int64_t)gridDim.x * blockDim.x) {
         const int32_t r = from[k];
-        deg[k] = rowptr[r + 1] - rowptr[r];
+        const int64_t s = rowptr[r];
+        deg[k] = rowptr[r + 1] - s;
+        src_start[k] = s;
     }
 }
 
-// new row k = old row from[k], tails renamed through `rename`, entry order kept;
-// eight lanes per row (rows are short)
-__global__ void k_move_rows(const int64_t *__restrict__ rp, const int32_t *__restrict__ tail,
-                            const double *__restrict__ w, int64_t n, const int32_t *__restrict__ from,
+// new row k = old row from[k] (starting at src_start[k]), tails renamed through
+// `rename`, entry order kept; eight lanes per row (rows are short), two entries per
+// lane per step: both tails are loaded before the renames are gathered
+__global__ void k_move_rows(const int32_t *__restrict__ tail, const double *__restrict__ w, int64_t n,
+                            const int64_t *__restrict__ src_start,
                             const int32_t *__restrict__ rename, const int64_t *__restrict__ rp2,
                             int32_t *__restrict__ tail2, double *__restrict__ w2) {
     const int sub = threadIdx.x & 7;
     const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
     const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
     for (int64_t k = grp; k < n; k += ng) {
-        const int32_t r = from[k];
-        const int64_t s = rp[r], len = rp[r + 1] - s, o = rp2[k];
-        for (int64_t j = sub; j < len; j += 8) {
-            tail2[o + j] = rename[tail[s + j]];
-            w2[o + j] = w[s + j];
+        const int64_t s = src_start[k], o = rp2[k], len = rp2[k + 1] - o;
+        for (int64_t j = sub; j < len; j += 16) {
+            const bool two = j + 8 < len;
+            const int32_t t0 = tail[s + j];
+            const int32_t t1 = two ? tail[s + j + 8] : 0;
+            const double w0 = w[s + j];
+            const double w1 = two ? w[s + j + 8] : 0.0;
+            const int32_t r0 = rename[t0];
+            const int32_t r1 = two ? rename[t1] : 0;
+            tail2[o + j] = r0;
+            w2[o + j] = w0;
+            if (two) {
+                tail2[o + j + 8] = r1;
+                w2[o + j + 8] = w1;
+            }
         }
     }
 }
@@ -241,11 +260,12 @@ bool vg_local_structure(vg_ctx *ctx, const vg_graph *g) {
 static vg_graph *move_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *from,
                            const int32_t *rename) {
     const int64_t nv = g->nv, ne = g->ne;
-    DevBuf<int64_t> rp(ctx, nv + 1);
+    DevBuf<int64_t> rp(ctx, nv + 1), src(ctx, nv);
     VG_CUDA(cudaMemsetAsync(rp.p + nv, 0, sizeof(int64_t), ctx->stream));
     if (nv) {
         LaunchTimer lt(ctx);
-        k_gather_deg<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(g->rowptr, from, nv, rp.p);
+        k_gather_deg<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(g->rowptr, from, nv, rp.p,
+                                                                     src.p);
     }
     VG_CHECK_LAUNCH();
     vg_scan_i64_async(ctx, rp.p, nv + 1, nullptr);
@@ -254,7 +274,7 @@ static vg_graph *move_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *from,
     if (nv) {
         LaunchTimer lt(ctx);
         k_move_rows<<<vg_grid(ctx, nv * 8, 256), 256, 0, ctx->stream>>>(
-            g->rowptr, g->tail, g->weight, nv, from, rename, rp.p, tail.p, w.p);
+            g->tail, g->weight, nv, src.p, rename, rp.p, tail.p, w.p);
     }
     VG_CHECK_LAUNCH();
     return vg_graph_wrap(ctx, nv, ne, rp.detach(), tail.detach(), w.detach());
