@@ -869,33 +869,59 @@ __device__ __forceinline__ double row_fold(const double *__restrict__ w, int64_t
     return sum;
 }
 
+// one lane per row for rows of at most DEG_LONG entries; longer rows are listed
+// (any order) for k_degree_long
 __global__ void k_degree(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
-                         int64_t nv, double *__restrict__ vdeg, int integral) {
+                         int64_t nv, double *__restrict__ vdeg, int32_t *__restrict__ long_rows,
+                         int64_t long_cap, unsigned long long *__restrict__ long_count) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e0 = rowptr[v], e1 = rowptr[v + 1];
+        if (e1 - e0 <= DEG_LONG) {
+            vdeg[v] = row_fold(w, e0, e1);
+        } else {
+            const unsigned long long s = atomicAdd(long_count, 1ULL);
+            if ((int64_t)s < long_cap) long_rows[s] = (int32_t)v;
+        }
+    }
+}
+
+// one warp per listed row. Integral weights: every partial sum is exact, so lanes
+// add strided entries and a shuffle tree combines them. Otherwise the row's left
+// fold in CSR order: the warp loads 32 consecutive weights (the next 32 in flight
+// meanwhile) and every lane adds them in lane order from broadcasts, so all lanes
+// hold the serial fold's bits.
+__global__ void k_degree_long(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
+                              double *__restrict__ vdeg, const int32_t *__restrict__ long_rows,
+                              int64_t long_cap, const unsigned long long *__restrict__ long_count,
+                              int integral) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    const int64_t n = min((int64_t)*long_count, long_cap);
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < nv;
-         base += nw * 32) {
-        const int64_t v = base + lane;
-        const bool valid = v < nv;
-        int64_t e0 = 0, e1 = 0;
-        if (valid) {
-            e0 = rowptr[v];
-            e1 = rowptr[v + 1];
-        }
-        const bool coop = integral && valid && e1 - e0 > DEG_LONG;
-        if (valid && !coop) vdeg[v] = row_fold(w, e0, e1);
-        unsigned lm = __ballot_sync(full, coop);
-        while (lm) {
-            const int src = __ffs(lm) - 1;
-            lm &= lm - 1;
-            const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
-            double sum = 0.0;
+    for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < n; q += nw) {
+        const int32_t v = long_rows[q];
+        const int64_t E0 = rowptr[v], E1 = rowptr[v + 1];
+        double sum = 0.0;
+        if (integral) {
             for (int64_t k = E0 + lane; k < E1; k += 32) sum = __dadd_rn(sum, w[k]);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) sum = __dadd_rn(sum, __shfl_xor_sync(full, sum, o));
-            if (lane == src) vdeg[v] = sum;
+        } else {
+            double x = E0 + lane < E1 ? w[E0 + lane] : 0.0;
+            for (int64_t base = E0; base < E1; base += 32) {
+                const int64_t kn = base + 32 + lane;
+                const double xn = kn < E1 ? w[kn] : 0.0;
+                const int cnt = (int)min((int64_t)32, E1 - base);
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const double y = __shfl_sync(full, x, j);
+                    if (j < cnt) sum = __dadd_rn(sum, y);
+                }
+                x = xn;
+            }
         }
+        if (lane == 0) vdeg[v] = sum;
     }
 }
 
@@ -1397,6 +1423,29 @@ static void configure_kernels_once() {
     done = true;
 }
 
+// vdeg[v] = the sum of v's row weights (distCalcVertexDegree, louvain.cpp:2118-2136):
+// short rows one per lane, rows longer than DEG_LONG one per warp
+static void vertex_degrees(vg_ctx *ctx, const vg_graph *g, double *vdeg, int integral) {
+    const int64_t nv = g->nv;
+    if (nv == 0) return;
+    const int64_t cap = std::min<int64_t>(nv, g->ne / (DEG_LONG + 1) + 1);
+    DevBuf<int32_t> list(ctx, cap);
+    DevBuf<unsigned long long> cnt(ctx, 1);
+    VG_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), ctx->stream));
+    {
+        LaunchTimer lt(ctx);
+        k_degree<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(g->rowptr, g->weight, nv, vdeg,
+                                                                 list.p, cap, cnt.p);
+    }
+    VG_CHECK_LAUNCH();
+    if (g->ne > DEG_LONG) {
+        LaunchTimer lt(ctx);
+        k_degree_long<<<vg_grid(ctx, cap * 32, 256, 8), 256, 0, ctx->stream>>>(
+            g->rowptr, g->weight, vdeg, list.p, cap, cnt.p, integral);
+    }
+    VG_CHECK_LAUNCH();
+}
+
 struct GlobalTable {
     DevBuf<int32_t> keys;
     DevBuf<double> vals;
@@ -1495,12 +1544,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
     }
     const int grid = vg_grid(ctx, nv, 256);
     if (nv) {
-        const int integ = (int)vg_weights_integral(ctx, g);
-        {
-            LaunchTimer lt(ctx);
-            k_degree<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->weight, nv, vdeg.p, integ);
-        }
-        VG_CHECK_LAUNCH();
+        vertex_degrees(ctx, g, vdeg.p, (int)vg_weights_integral(ctx, g));
     }
     const double twice_m = nv ? twice_m_one(ctx, vdeg.p, nv) : 0.0;
     const double constant = 1.0 / twice_m; // distCalcConstantForSecondTerm (louvain.cpp:2217)
@@ -1679,12 +1723,7 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
     DevBuf<CommInfo> cupd(ctx, nv);
     DevBuf<int32_t> B0(ctx, nv), B1(ctx, nv), B2(ctx, nv);
     const int grid = vg_grid(ctx, nv, 256);
-    const int integ = (int)vg_weights_integral(ctx, U);
-    {
-        LaunchTimer lt(ctx);
-        k_degree<<<grid, 256, 0, ctx->stream>>>(U->rowptr, U->weight, nv, vdeg.p, integ);
-    }
-    VG_CHECK_LAUNCH();
+    vertex_degrees(ctx, U, vdeg.p, (int)vg_weights_integral(ctx, U));
     // per-graph 2m in each graph's own fixed order, 1/(2m) on the host as in the plain path
     DevBuf<double> jconst(ctx, J);
     {
@@ -1915,13 +1954,7 @@ extern "C" vg_status vg_vertex_degree(vg_ctx *ctx, vg_graph *g, double *vdeg_out
     return vg_guard(ctx, [&] {
         VG_CUDA(cudaSetDevice(ctx->device));
         DevBuf<double> vdeg(ctx, g->nv);
-        if (g->nv) {
-            const int integ = (int)vg_weights_integral(ctx, g);
-            LaunchTimer lt(ctx);
-            k_degree<<<vg_grid(ctx, g->nv, 256), 256, 0, ctx->stream>>>(g->rowptr, g->weight, g->nv,
-                                                                         vdeg.p, integ);
-        }
-        VG_CHECK_LAUNCH();
+        if (g->nv) vertex_degrees(ctx, g, vdeg.p, (int)vg_weights_integral(ctx, g));
         const double tm = g->nv ? twice_m_one(ctx, vdeg.p, g->nv) : 0.0;
         if (constant_out) *constant_out = 1.0 / tm;
         if (vdeg_out && g->nv) {
