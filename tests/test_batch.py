@@ -69,6 +69,21 @@ def test_batch_real_weights_match_plain(ctx):
         g.free()
 
 
+def test_batch_with_hub_graph(ctx):
+    """A graph whose hubs take the multi-CTA hub class, batched with small graphs
+    (unit weights: identical to its own run)."""
+    from conftest import multi_hub_csr
+    rp, tl, w = multi_hub_csr(40000, 6, 6000, 23, False)
+    hub = ctx.upload(rp, tl, w)
+    gs = [ctx.generate_er(3000, 16.0, 5), hub, unit(ctx, ctx.generate_rgg(5000, 0.0, 0))]
+    ref = [plain(ctx, g) for g in gs]
+    out = ctx.run_batch(gs, want_comm=True)
+    for a, b in zip(out, ref):
+        assert_same(a, b, exact=True)
+    for g in gs:
+        g.free()
+
+
 def test_batch_with_locality_layout_graph(ctx):
     # n >= 2^18 takes the BFS locality layout in the plain path and in the batch
     big = unit(ctx, ctx.generate_rgg(1 << 18, 1.0, 13))

@@ -201,6 +201,41 @@ def test_phase_matches_oracle_with_hubs(ctx):
     assert float(mod).hex() == float(rmod).hex()
 
 
+@pytest.mark.parametrize("real", [False, True])
+def test_phase_many_hubs(ctx, real):
+    """Six hubs of degree ~6,000 (the hub class: rows spread over many CTAs, tables in
+    global memory) over a ring. Unit weights: bit-identical; U(0,1) weights: the hubs'
+    counters meet through FP64 atomics, so the same partition with the modularity
+    within 1e-9 relative."""
+    from conftest import multi_hub_csr
+    rp, tl, w = multi_hub_csr(40000, 6, 6000, 21, real)
+    ref = vo.Graph(rp, tl, w)
+    cv, mod, it = ctx.louvain_phase(upload(ctx, ref))
+    rcv, rmod, rit = vo.louvain_phase(ref)
+    assert it == rit
+    np.testing.assert_array_equal(cv, rcv)
+    if real:
+        assert abs(mod - rmod) <= REL_TOL * abs(rmod)
+    else:
+        assert float(mod).hex() == float(rmod).hex()
+
+
+def test_run_many_hubs_coloured_et(ctx):
+    """The hub class under coloring and early termination (`-c 8 -t 2 -a 0.25`) over
+    every level, against the oracle's run: same level sizes and iterations, the
+    modularity within 1e-9 relative (U(0,1) weights)."""
+    from conftest import multi_hub_csr
+    rp, tl, w = multi_hub_csr(40000, 6, 6000, 22, True)
+    ref = vo.Graph(rp, tl, w)
+    kw = vo.flags_to_kwargs(["-c", "8", "-t", "2", "-a", "0.25"])
+    res = ctx.run(upload(ctx, ref), **kw)
+    rr = vo.run(ref, **kw)
+    assert [s["nv"] for s in res.stats] == list(rr.level_nv)
+    assert [s["iters"] for s in res.stats] == list(rr.level_iters)
+    for s, rm in zip(res.stats, rr.level_mod):
+        assert abs(s["modularity"] - rm) <= REL_TOL * abs(rm)
+
+
 @pytest.mark.parametrize("n,m", [(20000, 8), (60000, 16)])
 def test_phase_ba_degree_classes(ctx, n, m):
     """BA graphs spread vertices over all degree classes (4..CTA)."""

@@ -23,23 +23,27 @@ __device__ __forceinline__ int32_t pos_of(const int32_t *__restrict__ pos, int64
     return pos ? pos[r] : (int32_t)r;
 }
 
+// vertices in reference order r, keyed by their new row; the payload is the
+// vertex's position, so the stable sort lists each row's vertices in reference
+// order by position
 __global__ void k_vertex_keys(int64_t nv, const int32_t *__restrict__ pos,
                               const int32_t *__restrict__ new_row, uint64_t *__restrict__ keys,
                               uint32_t *__restrict__ vals) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nv;
          r += (int64_t)gridDim.x * blockDim.x) {
-        keys[r] = (uint64_t)new_row[pos_of(pos, r)];
-        vals[r] = (uint32_t)r;
+        const int32_t p = pos_of(pos, r);
+        keys[r] = (uint64_t)new_row[p];
+        vals[r] = (uint32_t)p;
     }
 }
 
-// k-th vertex in grouped order: its degree, and where its row starts in the CSR
-__global__ void k_sorted_deg(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ pos,
-                             const uint32_t *__restrict__ order, int64_t nv, int64_t *__restrict__ deg,
-                             int64_t *__restrict__ src_start) {
+// k-th vertex in grouped order (order[k]: its position): its degree, and where its
+// row starts in the CSR
+__global__ void k_sorted_deg(const int64_t *__restrict__ rowptr, const uint32_t *__restrict__ order,
+                             int64_t nv, int64_t *__restrict__ deg, int64_t *__restrict__ src_start) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nv;
          k += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t p = pos_of(pos, order[k]);
+        const int32_t p = (int32_t)order[k];
         const int64_t e0 = rowptr[p];
         deg[k] = rowptr[p + 1] - e0;
         src_start[k] = e0;
@@ -515,7 +519,7 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     VG_CUDA(cudaMemsetAsync(off.p + nv, 0, sizeof(int64_t), ctx->stream));
     if (nv) {
         { LaunchTimer lt(ctx);
-          k_sorted_deg<<<grid, 256, 0, ctx->stream>>>(g->rowptr, pos, vorder.p, nv, off.p,
+          k_sorted_deg<<<grid, 256, 0, ctx->stream>>>(g->rowptr, vorder.p, nv, off.p,
                                                       src_start.p); }
         VG_CHECK_LAUNCH();
     }

@@ -23,7 +23,7 @@ namespace {
 constexpr int NCLS = 6;
 // class by degree: 0: <= TMAX (one thread per vertex) 1: <= 32 (one thread per vertex)
 // 2: <= WS_MAXDEG (warp, small shared-memory table) 3: <= WT_MAXDEG (warp, large
-// table) 4: <= CT_MAXDEG (CTA, shared table) 5: above (CTA, table in global scratch)
+// table) 4: <= CT_MAXDEG (CTA, shared table) 5: above (hubs, spread over many CTAs)
 constexpr int TMAX = 16;
 constexpr int TB = 256;
 #ifndef VG_WS_MAXDEG
@@ -37,6 +37,9 @@ constexpr int TB = 256;
 #endif
 #ifndef VG_T32
 #define VG_T32 1
+#endif
+#ifndef VG_T16_MINB
+#define VG_T16_MINB 3 // resident CTAs per SM of the degree-<=16 list kernel (coloured sweeps)
 #endif
 #ifndef VG_T32_MINB
 #define VG_T32_MINB 4 // resident CTAs per SM the degree-<=32 list kernel is sized for
@@ -178,7 +181,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // occurrence. Candidate degrees are gathered eight at a time.
 
 template <bool LIST, int T, int NT>
-__global__ void __launch_bounds__(NT, (T <= 16 ? 3 : VG_T32_MINB)) k_sweep_thread(
+__global__ void __launch_bounds__(NT, (T <= 16 ? VG_T16_MINB : VG_T32_MINB)) k_sweep_thread(
     SweepArgs a, const int32_t *__restrict__ list, int64_t count) {
     __shared__ double ssum[T][NT];
     const int tid = threadIdx.x;
@@ -646,24 +649,15 @@ struct CtaShared {
     double counter0;
 };
 
-template <bool GLOBAL_TABLE>
 __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int32_t *__restrict__ list,
-                                                          int64_t count, int32_t *__restrict__ gkeys,
-                                                          double *__restrict__ gvals, int64_t gcap) {
+                                                          int64_t count) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ CtaShared sh;
     __shared__ __align__(16) double stage[CT_THREADS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
-    double *vals;
-    int32_t *keys;
-    if (GLOBAL_TABLE) {
-        vals = gvals + (size_t)blockIdx.x * gcap;
-        keys = gkeys + (size_t)blockIdx.x * gcap;
-    } else {
-        vals = reinterpret_cast<double *>(smem_raw);
-        keys = reinterpret_cast<int32_t *>(vals + CT_CAP);
-    }
+    double *vals = reinterpret_cast<double *>(smem_raw);
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + CT_CAP);
     for (int64_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
         const int32_t v = list[idx];
         double cst;
@@ -843,6 +837,296 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
             commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, cand, csz);
         }
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// class 5 (degree > CT_MAXDEG, the hubs): every hub's row is spread over many CTAs.
+// Each hub owns a hash table in global memory (capacity the power of two >= twice its
+// degree, so at most half full). k_hub_accum: work items are chunks of HUB_CHUNK
+// entries of any hub; inside a warp's 32 entries the leader of each community folds
+// its lanes in lane order and the warps meet in the table through atomics (as the
+// CTA class does for its slices). k_hub_c0: the current community's counter.
+// k_hub_eval: work items are slices of HUB_SLICE table slots; each slice reports
+// its best (gain, id) and clears its slots for the next sweep. k_hub_commit: a warp
+// per hub picks the best of its slices (the (gain, id) order makes the choice
+// independent of the slices' order) and commits the move.
+
+constexpr int HUB_CHUNK = 4096;
+constexpr int HUB_SLICE = 4096;
+constexpr int HUB_THREADS = 256;
+
+struct HubBest {
+    double g;
+    int32_t c, sz;
+    int32_t ok, pad;
+};
+
+// largest q in [q0, q1) with pre[q] <= x (pre nondecreasing, pre[q0] <= x)
+__device__ __forceinline__ int64_t hub_owner(const int64_t *__restrict__ pre, int64_t q0, int64_t q1,
+                                             int64_t x) {
+    int64_t lo = q0, hi = q1;
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (pre[mid] <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ bool hub_swept(const SweepArgs &a, int32_t v, double &cst) {
+    return vertex_live(a, v, cst) && !(a.active && !a.active[v]);
+}
+
+__global__ void __launch_bounds__(HUB_THREADS) k_hub_accum(
+    SweepArgs a, const int32_t *__restrict__ vtx, const int64_t *__restrict__ toff,
+    const int64_t *__restrict__ cb, int64_t q0, int64_t q1, int32_t *__restrict__ keys,
+    double *__restrict__ vals, double *__restrict__ self) {
+    __shared__ __align__(16) double stage[HUB_THREADS];
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    double *st = stage + (threadIdx.x & ~31);
+    for (int64_t c = cb[q0] + blockIdx.x; c < cb[q1]; c += gridDim.x) {
+        const int64_t q = hub_owner(cb, q0, q1, c);
+        const int32_t v = vtx[q];
+        double cst;
+        if (!hub_swept(a, v, cst)) continue; // uniform over the block
+        const int64_t r0 = a.rowptr[v], r1 = a.rowptr[v + 1];
+        const int64_t e0 = r0 + (c - cb[q]) * HUB_CHUNK, e1 = min(e0 + HUB_CHUNK, r1);
+        const int64_t cap = toff[q + 1] - toff[q];
+        int logcap = 0;
+        while (((int64_t)1 << logcap) < cap) logcap++;
+        int32_t *hk = keys + toff[q];
+        double *hv = vals + toff[q];
+        double selfsum = 0.0;
+        bool anyself = false;
+        for (int64_t base = e0; base < e1; base += HUB_THREADS) {
+            const int64_t e = base + threadIdx.x;
+            const bool has = e < e1;
+            int32_t t = -1, cm = -1;
+            double w = 0.0;
+            if (has) {
+                t = a.tail[e];
+                w = a.weight[e];
+                cm = a.curr[t];
+            }
+            st[lane] = w;
+            const unsigned peers = __match_any_sync(full, has ? cm : (-1 - lane));
+            __syncwarp();
+            if (has && lane == __ffs(peers) - 1) {
+                double acc = w;
+                const unsigned above = peers & ~((2u << lane) - 1u);
+                if (above) acc = vg_fold_above(acc, st, above);
+                uint32_t h = slot_hash(cm, logcap);
+                for (;;) {
+                    const int32_t kk = hk[h];
+                    if (kk == cm) break;
+                    if (kk == EMPTY) {
+                        const int32_t old = atomicCAS(&hk[h], EMPTY, cm);
+                        if (old == EMPTY || old == cm) break;
+                    }
+                    h = (h + 1) & (uint32_t)(cap - 1);
+                }
+                atomicAdd(&hv[h], acc);
+            }
+            unsigned m = __ballot_sync(full, has && t == v);
+            anyself |= m != 0;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                selfsum = __dadd_rn(selfsum, st[b]);
+                m &= m - 1;
+            }
+            __syncwarp();
+        }
+        if (lane == 0 && anyself) atomicAdd(&self[q], selfsum);
+    }
+}
+
+__global__ void k_hub_c0(SweepArgs a, const int32_t *__restrict__ vtx, const int64_t *__restrict__ toff,
+                         int64_t q0, int64_t q1, const int32_t *__restrict__ keys,
+                         const double *__restrict__ vals, double *__restrict__ c0) {
+    for (int64_t q = q0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < q1;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = vtx[q];
+        double cst;
+        if (!hub_swept(a, v, cst)) continue;
+        const int32_t cc = a.curr[v];
+        const int64_t cap = toff[q + 1] - toff[q];
+        int logcap = 0;
+        while (((int64_t)1 << logcap) < cap) logcap++;
+        const int32_t *hk = keys + toff[q];
+        double x = 0.0;
+        uint32_t h = slot_hash(cc, logcap);
+        for (int64_t probe = 0; probe < cap; probe++) {
+            const int32_t kk = hk[h];
+            if (kk == cc) {
+                x = vals[toff[q] + h];
+                break;
+            }
+            if (kk == EMPTY) break;
+            h = (h + 1) & (uint32_t)(cap - 1);
+        }
+        c0[q] = x;
+    }
+}
+
+__global__ void __launch_bounds__(HUB_THREADS) k_hub_eval(
+    SweepArgs a, const int32_t *__restrict__ vtx, const int64_t *__restrict__ toff,
+    const int64_t *__restrict__ sb, int64_t q0, int64_t q1, int32_t *__restrict__ keys,
+    double *__restrict__ vals, const double *__restrict__ self, const double *__restrict__ c0,
+    HubBest *__restrict__ best) {
+    __shared__ double red_g[HUB_THREADS / 32];
+    __shared__ int32_t red_c[HUB_THREADS / 32], red_s[HUB_THREADS / 32], red_ok[HUB_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned full = 0xffffffffu;
+    for (int64_t sl = sb[q0] + blockIdx.x; sl < sb[q1]; sl += gridDim.x) {
+        const int64_t q = hub_owner(sb, q0, q1, sl);
+        const int32_t v = vtx[q];
+        double cst;
+        if (!hub_swept(a, v, cst)) continue; // its table was left empty
+        const int32_t cc = a.curr[v];
+        const double vd = a.vdeg[v];
+        const double eix = __dsub_rn(c0[q], self[q]);
+        const double ax = __dsub_rn(__ldg(a.cdeg + cc), vd);
+        const int64_t s0 = toff[q] + (sl - sb[q]) * HUB_SLICE;
+        double gain = 0.0;
+        int32_t cand = INT_MAX, csz = 0;
+        bool ok = false;
+        // four slots per thread per round, their community loads issued together
+        for (int64_t r = 0; r < HUB_SLICE; r += 4 * HUB_THREADS) {
+            int32_t kq[4], sq[4];
+            double vq[4], aq[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int64_t sidx = s0 + r + j * HUB_THREADS + threadIdx.x;
+                kq[j] = keys[sidx];
+                vq[j] = vals[sidx];
+                if (kq[j] != EMPTY) {
+                    keys[sidx] = EMPTY; // clean for the next sweep
+                    vals[sidx] = 0.0;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                aq[j] = 0.0;
+                sq[j] = 0;
+                if (kq[j] != EMPTY && kq[j] != cc) load_comm(a, kq[j], aq[j], sq[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (kq[j] == EMPTY || kq[j] == cc) continue;
+                const double g = gain_of(vq[j], eix, vd, aq[j], ax, cst);
+                if (g > 0.0 && better(true, g, kq[j], ok, gain, cand, a.ref)) {
+                    gain = g;
+                    cand = kq[j];
+                    csz = sq[j];
+                    ok = true;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double og = __shfl_xor_sync(full, gain, o);
+            const int32_t oc = __shfl_xor_sync(full, cand, o);
+            const int32_t os = __shfl_xor_sync(full, csz, o);
+            const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
+            if (better(ook, og, oc, ok, gain, cand, a.ref)) {
+                gain = og;
+                cand = oc;
+                csz = os;
+                ok = true;
+            }
+        }
+        if (lane == 0) {
+            red_g[warp] = gain;
+            red_c[warp] = cand;
+            red_s[warp] = csz;
+            red_ok[warp] = ok;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < HUB_THREADS / 32; w++) {
+                if (better(red_ok[w] != 0, red_g[w], red_c[w], ok, gain, cand, a.ref)) {
+                    gain = red_g[w];
+                    cand = red_c[w];
+                    csz = red_s[w];
+                    ok = true;
+                }
+            }
+            HubBest b;
+            b.g = gain;
+            b.c = cand;
+            b.sz = csz;
+            b.ok = ok;
+            b.pad = 0;
+            best[sl] = b;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_hub_commit(SweepArgs a, const int32_t *__restrict__ vtx, const int64_t *__restrict__ sb,
+                             int64_t q0, int64_t q1, double *__restrict__ self,
+                             const double *__restrict__ c0, const HubBest *__restrict__ best) {
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t q = q0 + ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5); q < q1; q += nw) {
+        const int32_t v = vtx[q];
+        double cst;
+        if (!vertex_live(a, v, cst)) continue;
+        if (a.active && !a.active[v]) {
+            if (lane == 0) a.cw[v] = a.frozen[v];
+            continue;
+        }
+        double gain = 0.0;
+        int32_t cand = INT_MAX, csz = 0;
+        bool ok = false;
+        for (int64_t sl = sb[q] + lane; sl < sb[q + 1]; sl += 32) {
+            const HubBest b = best[sl];
+            if (better(b.ok != 0, b.g, b.c, ok, gain, cand, a.ref)) {
+                gain = b.g;
+                cand = b.c;
+                csz = b.sz;
+                ok = true;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double og = __shfl_xor_sync(full, gain, o);
+            const int32_t oc = __shfl_xor_sync(full, cand, o);
+            const int32_t os = __shfl_xor_sync(full, csz, o);
+            const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
+            if (better(ook, og, oc, ok, gain, cand, a.ref)) {
+                gain = og;
+                cand = oc;
+                csz = os;
+                ok = true;
+            }
+        }
+        if (lane == 0) {
+            const int32_t cc = a.curr[v];
+            const int32_t ccSize = __ldg(a.csize + cc);
+            commit_vertex(a, v, cc, ccSize, a.vdeg[v], true, c0[q], ok, cand, csz);
+            self[q] = 0.0; // for the next sweep
+        }
+    }
+}
+
+// per listed hub: its degree -> table capacity, accumulation chunks, evaluation slices
+__global__ void k_hub_plan(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ list,
+                           int64_t n, int32_t *__restrict__ vtx, int64_t *__restrict__ cap,
+                           int64_t *__restrict__ chunks, int64_t *__restrict__ slices) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = list[q];
+        const int64_t d = rowptr[v + 1] - rowptr[v];
+        int64_t c = HUB_SLICE;
+        while (c < 2 * d) c <<= 1;
+        vtx[q] = v;
+        cap[q] = c;
+        chunks[q] = (d + HUB_CHUNK - 1) / HUB_CHUNK;
+        slices[q] = c / HUB_SLICE;
     }
 }
 
@@ -1254,26 +1538,18 @@ __device__ __forceinline__ int32_t bucket_key(const int64_t *__restrict__ rowptr
 // adds its counts to the global ones (one atomic per bucket per block).
 __global__ void k_bucket_count(const int64_t *__restrict__ rowptr, int64_t nv,
                                const int32_t *__restrict__ colors, int64_t numColor, int nb,
-                               int64_t chunk, int32_t *__restrict__ counts,
-                               unsigned long long *__restrict__ maxdeg) {
+                               int64_t chunk, int32_t *__restrict__ counts) {
     extern __shared__ int32_t sc[];
-    __shared__ unsigned long long smax;
     for (int k = threadIdx.x; k < nb; k += blockDim.x) sc[k] = 0;
-    if (threadIdx.x == 0) smax = 0;
     __syncthreads();
     const int64_t b0 = blockIdx.x * chunk, b1 = min(nv, b0 + chunk);
-    unsigned long long mx = 0;
     for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
         int64_t d;
-        const int32_t k = bucket_key(rowptr, i, colors, numColor, &d);
-        atomicAdd(&sc[k], 1);
-        if (d > CT_MAXDEG && (unsigned long long)d > mx) mx = (unsigned long long)d;
+        atomicAdd(&sc[bucket_key(rowptr, i, colors, numColor, &d)], 1);
     }
-    if (mx) atomicMax(&smax, mx);
     __syncthreads();
     for (int k = threadIdx.x; k < nb; k += blockDim.x)
         if (sc[k]) atomicAdd(&counts[k], sc[k]);
-    if (threadIdx.x == 0 && smax) atomicMax(maxdeg, smax);
 }
 
 // Each block reserves a range per bucket with one atomic and places its vertices
@@ -1357,7 +1633,6 @@ struct Buckets {
     DevBuf<int32_t> list;
     std::vector<int64_t> start; // (numColor * NCLS) + 1 offsets
     int64_t ncolor = 1;
-    int64_t maxdeg_global = 0;  // largest degree of the global-table class
 };
 
 static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors, int64_t numColor,
@@ -1367,24 +1642,19 @@ static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors,
     VG_REQUIRE(nb <= 6000, "too many color buckets (%lld colors)", (long long)numColor);
     b.ncolor = numColor;
     DevBuf<int32_t> counts(ctx, nb);
-    DevBuf<unsigned long long> maxdeg(ctx, 1);
     VG_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int32_t) * nb, ctx->stream));
-    VG_CUDA(cudaMemsetAsync(maxdeg.p, 0, sizeof(unsigned long long), ctx->stream));
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nv + 1023) / 1024, 4LL * ctx->sm_count));
     const int64_t chunk = (nv + blocks - 1) / blocks;
     if (nv) {
         LaunchTimer lt(ctx);
         k_bucket_count<<<blocks, 256, sizeof(int32_t) * nb, ctx->stream>>>(
-            g->rowptr, nv, colors, numColor, (int)nb, chunk, counts.p, maxdeg.p);
+            g->rowptr, nv, colors, numColor, (int)nb, chunk, counts.p);
     }
     VG_CHECK_LAUNCH();
     std::vector<int32_t> hc(nb);
-    unsigned long long hmax = 0;
     VG_CUDA(cudaMemcpyAsync(hc.data(), counts.p, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost,
                             ctx->stream));
-    VG_CUDA(cudaMemcpyAsync(&hmax, maxdeg.p, sizeof(hmax), cudaMemcpyDeviceToHost, ctx->stream));
     vg_sync(ctx);
-    b.maxdeg_global = (int64_t)hmax;
     b.start.assign(nb + 1, 0);
     std::vector<int32_t> fill(nb);
     for (int64_t k = 0; k < nb; k++) {
@@ -1418,7 +1688,7 @@ static void configure_kernels_once() {
     VG_CUDA(cudaFuncSetAttribute(k_sweep_warp<WT_CAP, WT_WARPS>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)warp_smem_bytes<WT_CAP, WT_WARPS>()));
-    VG_CUDA(cudaFuncSetAttribute(k_sweep_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    VG_CUDA(cudaFuncSetAttribute(k_sweep_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_smem_bytes()));
     done = true;
 }
@@ -1446,17 +1716,104 @@ static void vertex_degrees(vg_ctx *ctx, const vg_graph *g, double *vdeg, int int
     VG_CHECK_LAUNCH();
 }
 
-struct GlobalTable {
+// The hubs (class 5) of every color, planned once per phase: plan index q runs over
+// the colors' class-5 lists in color order; color k owns [first[k], first[k+1]).
+struct HubPlan {
+    int64_t n = 0;
+    std::vector<int64_t> first;    // numColor + 1
+    std::vector<int64_t> hcb, hsb; // host copies of the chunk and slice prefixes (n + 1)
+    DevBuf<int32_t> vtx;
+    DevBuf<int64_t> toff, cb, sb;
     DevBuf<int32_t> keys;
-    DevBuf<double> vals;
-    int64_t cap = 0;
-    int blocks = 0;
+    DevBuf<double> vals, self, c0;
+    DevBuf<HubBest> best;
 };
+
+static void plan_hubs(vg_ctx *ctx, const vg_graph *g, const Buckets &bk, int64_t numColor,
+                      HubPlan &hp) {
+    hp.first.assign(numColor + 1, 0);
+    for (int64_t k = 0; k < numColor; k++)
+        hp.first[k + 1] = hp.first[k] + (bk.start[k * NCLS + 6] - bk.start[k * NCLS + 5]);
+    hp.n = hp.first[numColor];
+    if (hp.n == 0) return;
+    const int64_t n = hp.n;
+    hp.vtx.alloc(ctx, n);
+    hp.toff.alloc(ctx, n + 1);
+    hp.cb.alloc(ctx, n + 1);
+    hp.sb.alloc(ctx, n + 1);
+    VG_CUDA(cudaMemsetAsync(hp.toff.p + n, 0, sizeof(int64_t), ctx->stream));
+    VG_CUDA(cudaMemsetAsync(hp.cb.p + n, 0, sizeof(int64_t), ctx->stream));
+    VG_CUDA(cudaMemsetAsync(hp.sb.p + n, 0, sizeof(int64_t), ctx->stream));
+    for (int64_t k = 0; k < numColor; k++) {
+        const int64_t m = hp.first[k + 1] - hp.first[k];
+        if (m == 0) continue;
+        const int64_t q = hp.first[k];
+        LaunchTimer lt(ctx);
+        k_hub_plan<<<vg_grid(ctx, m, 256), 256, 0, ctx->stream>>>(
+            g->rowptr, bk.list.p + bk.start[k * NCLS + 5], m, hp.vtx.p + q, hp.toff.p + q,
+            hp.cb.p + q, hp.sb.p + q);
+        VG_CHECK_LAUNCH();
+    }
+    vg_scan_i64_async(ctx, hp.toff.p, n + 1, nullptr);
+    vg_scan_i64_async(ctx, hp.cb.p, n + 1, nullptr);
+    vg_scan_i64_async(ctx, hp.sb.p, n + 1, nullptr);
+    hp.hcb.resize(n + 1);
+    hp.hsb.resize(n + 1);
+    int64_t slots = 0;
+    VG_CUDA(cudaMemcpyAsync(hp.hcb.data(), hp.cb.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    VG_CUDA(cudaMemcpyAsync(hp.hsb.data(), hp.sb.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    VG_CUDA(cudaMemcpyAsync(&slots, hp.toff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    vg_sync(ctx);
+    hp.keys.alloc(ctx, slots);
+    hp.vals.alloc(ctx, slots);
+    hp.self.alloc(ctx, n);
+    hp.c0.alloc(ctx, n);
+    hp.best.alloc(ctx, hp.hsb[n]);
+    VG_CUDA(cudaMemsetAsync(hp.keys.p, 0xff, sizeof(int32_t) * slots, ctx->stream)); // EMPTY
+    VG_CUDA(cudaMemsetAsync(hp.vals.p, 0, sizeof(double) * slots, ctx->stream));
+    VG_CUDA(cudaMemsetAsync(hp.self.p, 0, sizeof(double) * n, ctx->stream));
+}
+
+// one sweep over the hubs of color k
+static void sweep_hubs(vg_ctx *ctx, const SweepArgs &a, HubPlan &hp, int64_t k) {
+    const int64_t q0 = hp.first[k], q1 = hp.first[k + 1];
+    if (q1 == q0) return;
+    const int64_t nch = hp.hcb[q1] - hp.hcb[q0], nsl = hp.hsb[q1] - hp.hsb[q0];
+    const int64_t cap_blocks = 8LL * ctx->sm_count;
+    {
+        LaunchTimer lt(ctx);
+        k_hub_accum<<<(int)std::min(nch, cap_blocks), HUB_THREADS, 0, ctx->stream>>>(
+            a, hp.vtx.p, hp.toff.p, hp.cb.p, q0, q1, hp.keys.p, hp.vals.p, hp.self.p);
+    }
+    VG_CHECK_LAUNCH();
+    {
+        LaunchTimer lt(ctx);
+        k_hub_c0<<<vg_grid(ctx, q1 - q0, 256), 256, 0, ctx->stream>>>(
+            a, hp.vtx.p, hp.toff.p, q0, q1, hp.keys.p, hp.vals.p, hp.c0.p);
+    }
+    VG_CHECK_LAUNCH();
+    {
+        LaunchTimer lt(ctx);
+        k_hub_eval<<<(int)std::min(nsl, cap_blocks), HUB_THREADS, 0, ctx->stream>>>(
+            a, hp.vtx.p, hp.toff.p, hp.sb.p, q0, q1, hp.keys.p, hp.vals.p, hp.self.p, hp.c0.p,
+            hp.best.p);
+    }
+    VG_CHECK_LAUNCH();
+    {
+        LaunchTimer lt(ctx);
+        k_hub_commit<<<vg_grid(ctx, (q1 - q0) * 32, 256), 256, 0, ctx->stream>>>(
+            a, hp.vtx.p, hp.sb.p, q0, q1, hp.self.p, hp.c0.p, hp.best.p);
+    }
+    VG_CHECK_LAUNCH();
+}
 
 // launch the sweep kernels over one color bucket; with `natural` the low-degree
 // class runs over all vertices in id order instead of its list
 static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64_t color,
-                        GlobalTable &gt, bool natural, int64_t nv) {
+                        HubPlan &hp, bool natural, int64_t nv) {
     const int32_t *list = b.list.p;
     for (int cls = 0; cls < NCLS; cls++) {
         const int64_t s = b.start[color * NCLS + cls], e = b.start[color * NCLS + cls + 1];
@@ -1470,6 +1827,10 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
             continue;
         }
         if (n == 0) continue;
+        if (cls == NCLS - 1) { // the hubs
+            sweep_hubs(ctx, a, hp, color);
+            continue;
+        }
         LaunchTimer lt(ctx);
         switch (cls) {
         case 0:
@@ -1489,14 +1850,11 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
                 a, list + s, n);
             break;
         case 4:
-            k_sweep_cta<false><<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, 2), CT_THREADS,
-                                 cta_smem_bytes(), ctx->stream>>>(a, list + s, n, nullptr, nullptr, 0);
+            k_sweep_cta<<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, 2), CT_THREADS, cta_smem_bytes(),
+                          ctx->stream>>>(a, list + s, n);
             break;
-        default: {
-            const int blocks = (int)std::min<int64_t>(n, gt.blocks);
-            k_sweep_cta<true><<<blocks, CT_THREADS, 0, ctx->stream>>>(a, list + s, n, gt.keys.p,
-                                                                      gt.vals.p, gt.cap);
-        }
+        default:
+            break;
         }
         VG_CHECK_LAUNCH();
     }
@@ -1556,18 +1914,8 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
     VG_CHECK_LAUNCH();
     Buckets bk;
     build_buckets(ctx, g, ordering ? g->colors : nullptr, numColor, bk);
-    GlobalTable gt;
-    if (bk.maxdeg_global > 0) {
-        int64_t cap = 32;
-        while (cap < 2 * bk.maxdeg_global) cap <<= 1;
-        int64_t n6 = 0;
-        for (int64_t c = 0; c < numColor; c++)
-            n6 = std::max(n6, bk.start[c * NCLS + 6] - bk.start[c * NCLS + 5]);
-        gt.blocks = (int)std::min<int64_t>(n6, (int64_t)ctx->sm_count * 2);
-        gt.cap = cap;
-        gt.keys.alloc(ctx, (size_t)cap * gt.blocks);
-        gt.vals.alloc(ctx, (size_t)cap * gt.blocks);
-    }
+    HubPlan hp;
+    plan_hubs(ctx, g, bk, numColor, hp);
     SegTable seg;
     {
         const int64_t voff[2] = {0, nv};
@@ -1608,7 +1956,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         a.constant = constant;
         if (timing) VG_CUDA(cudaEventRecord(ev0, ctx->stream));
         for (int64_t ci = 0; ci < numColor; ci++) {
-            sweep_color(ctx, a, bk, ci, gt, ordering == 0, nv);
+            sweep_color(ctx, a, bk, ci, hp, ordering == 0, nv);
             if (ordering == 1 && nv) { // per-color community update (louvain.cpp:724-735)
                 LaunchTimer lt(ctx);
                 k_apply_seg<<<agrid, SEG_THREADS, 0, ctx->stream>>>(
@@ -1746,16 +2094,8 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
     VG_CHECK_LAUNCH();
     Buckets bk;
     build_buckets(ctx, U, nullptr, 1, bk);
-    GlobalTable gt;
-    if (bk.maxdeg_global > 0) {
-        int64_t cap = 32;
-        while (cap < 2 * bk.maxdeg_global) cap <<= 1;
-        const int64_t n6 = bk.start[5] - bk.start[4];
-        gt.blocks = (int)std::min<int64_t>(n6, (int64_t)ctx->sm_count * 2);
-        gt.cap = cap;
-        gt.keys.alloc(ctx, (size_t)cap * gt.blocks);
-        gt.vals.alloc(ctx, (size_t)cap * gt.blocks);
-    }
+    HubPlan hp;
+    plan_hubs(ctx, U, bk, 1, hp);
     DevBuf<double> part(ctx, 3 * std::max<int64_t>(seg.C, 1));
     const int agrid = seg_grid(ctx, seg.C);
     // per-graph loop state
@@ -1796,7 +2136,7 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
         a.jdone = done.p;
         VG_CUDA(cudaMemsetAsync(live.p, 0, sizeof(int32_t), ctx->stream));
         if (e0) VG_CUDA(cudaEventRecord(e0, ctx->stream));
-        sweep_color(ctx, a, bk, 0, gt, true, nv);
+        sweep_color(ctx, a, bk, 0, hp, true, nv);
         if (e1) VG_CUDA(cudaEventRecord(e1, ctx->stream));
         {
             LaunchTimer lt(ctx);

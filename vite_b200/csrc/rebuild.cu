@@ -31,19 +31,32 @@ __global__ void k_first_member(const int32_t *__restrict__ comm, int64_t nv,
         atomicMin(&first[comm[i]], (int32_t)i);
 }
 
-__global__ void k_first_flag(const int32_t *__restrict__ comm, int64_t nv,
-                             const int32_t *__restrict__ first, int32_t *__restrict__ flag) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
-         i += (int64_t)gridDim.x * blockDim.x)
-        flag[i] = first[comm[i]] == (int32_t)i ? 1 : 0;
+// per community slot c with members (first[c] set): flag its first member, in the
+// order the flags are indexed by
+__global__ void k_comm_flag(const int32_t *__restrict__ first, int64_t n, int32_t *__restrict__ flag) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t f = first[c];
+        if (f != INT_MAX) flag[f] = 1;
+    }
 }
 
-__global__ void k_new_of(const int32_t *__restrict__ comm, int64_t nv,
-                         const int32_t *__restrict__ first, const int64_t *__restrict__ rank,
+// per community slot: its new id, the rank of its first member among the flagged
+// ones (in place over first[])
+__global__ void k_comm_rank(int32_t *__restrict__ first, int64_t n, const int64_t *__restrict__ rank) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t f = first[c];
+        if (f != INT_MAX) first[c] = (int32_t)rank[f];
+    }
+}
+
+// per vertex: the new id of its community
+__global__ void k_new_of(const int32_t *__restrict__ comm, int64_t nv, const int32_t *__restrict__ cid,
                          int32_t *__restrict__ newof) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
          i += (int64_t)gridDim.x * blockDim.x)
-        newof[i] = (int32_t)rank[first[comm[i]]];
+        newof[i] = cid[comm[i]];
 }
 
 // one warp per row: triples in CSR order with coalesced writes
@@ -74,43 +87,60 @@ __global__ void k_triples(const int64_t *__restrict__ rowptr, const int32_t *__r
 // emitted in reference vertex order, so equal pairs fold in the reference's order.
 namespace {
 
-__global__ void k_first_ref(const int32_t *__restrict__ comm, int64_t nv,
-                            const int32_t *__restrict__ ref, int32_t *__restrict__ first) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nv;
-         p += (int64_t)gridDim.x * blockDim.x)
-        atomicMin(&first[comm[p]], ref[p]);
-}
-
-// flag_ref[r] = 1 where r is the first (smallest-reference-id) member of its
-// community; flag_pos[p] likewise by position
-__global__ void k_first_flags(const int32_t *__restrict__ comm, int64_t nv,
-                              const int32_t *__restrict__ ref, const int32_t *__restrict__ first_ref,
-                              const int32_t *__restrict__ first_pos, int32_t *__restrict__ flag_ref,
-                              int32_t *__restrict__ flag_pos) {
+// both first members of each community: smallest reference id and smallest position
+__global__ void k_first_both(const int32_t *__restrict__ comm, int64_t nv,
+                             const int32_t *__restrict__ ref, int32_t *__restrict__ first_ref,
+                             int32_t *__restrict__ first_pos) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nv;
          p += (int64_t)gridDim.x * blockDim.x) {
         const int32_t c = comm[p];
-        flag_ref[ref[p]] = first_ref[c] == ref[p] ? 1 : 0;
-        flag_pos[p] = first_pos[c] == (int32_t)p ? 1 : 0;
+        atomicMin(&first_ref[c], ref[p]);
+        atomicMin(&first_pos[c], (int32_t)p);
     }
 }
 
-__global__ void k_new_ids(const int32_t *__restrict__ comm, int64_t nv,
-                          const int32_t *__restrict__ first_ref, const int64_t *__restrict__ rank_ref,
-                          const int32_t *__restrict__ first_pos, const int64_t *__restrict__ rank_pos,
-                          int32_t *__restrict__ new_ref, int32_t *__restrict__ new_pos,
-                          int32_t *__restrict__ next_ref, int32_t *__restrict__ next_pos) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nv;
-         p += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t c = comm[p];
-        const int32_t nr = (int32_t)rank_ref[first_ref[c]];
-        const int32_t np = (int32_t)rank_pos[first_pos[c]];
-        new_ref[p] = nr;
-        new_pos[p] = np;
-        if (first_pos[c] == (int32_t)p) {
+// per community slot with members: flag_ref at its first reference id, flag_pos at
+// its first position
+__global__ void k_comm_flags(const int32_t *__restrict__ first_ref, const int32_t *__restrict__ first_pos,
+                             int64_t n, int32_t *__restrict__ flag_ref, int32_t *__restrict__ flag_pos) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t fp = first_pos[c];
+        if (fp != INT_MAX) {
+            flag_ref[first_ref[c]] = 1;
+            flag_pos[fp] = 1;
+        }
+    }
+}
+
+// per community slot with members: its next-level reference id nr and position np
+// (in place over first_ref / first_pos), and the next level's ref/pos maps
+__global__ void k_comm_ids(int32_t *__restrict__ first_ref, int32_t *__restrict__ first_pos, int64_t n,
+                           const int64_t *__restrict__ rank_ref, const int64_t *__restrict__ rank_pos,
+                           int32_t *__restrict__ next_ref, int32_t *__restrict__ next_pos) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t fp = first_pos[c];
+        if (fp != INT_MAX) {
+            const int32_t nr = (int32_t)rank_ref[first_ref[c]];
+            const int32_t np = (int32_t)rank_pos[fp];
+            first_ref[c] = nr;
+            first_pos[c] = np;
             next_ref[np] = nr;
             next_pos[nr] = np;
         }
+    }
+}
+
+// per vertex: its community's next-level reference id and position
+__global__ void k_vertex_ids(const int32_t *__restrict__ comm, int64_t nv,
+                             const int32_t *__restrict__ cnr, const int32_t *__restrict__ cnp,
+                             int32_t *__restrict__ new_ref, int32_t *__restrict__ new_pos) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nv;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t c = comm[p];
+        new_ref[p] = cnr[c];
+        new_pos[p] = cnp[c];
     }
 }
 
@@ -133,10 +163,13 @@ vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm) {
             VG_CHECK_LAUNCH();
             { LaunchTimer lt(ctx); k_first_member<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p); }
             VG_CHECK_LAUNCH();
-            { LaunchTimer lt(ctx); k_first_flag<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p, flag.p); }
+            VG_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int32_t) * nv, ctx->stream));
+            { LaunchTimer lt(ctx); k_comm_flag<<<grid, 256, 0, ctx->stream>>>(first.p, nv, flag.p); }
             VG_CHECK_LAUNCH();
             nc = vg_exclusive_scan_i32_to_i64(ctx, flag.p, rank.p, nv);
-            { LaunchTimer lt(ctx); k_new_of<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p, rank.p, newof.p); }
+            { LaunchTimer lt(ctx); k_comm_rank<<<grid, 256, 0, ctx->stream>>>(first.p, nv, rank.p); }
+            VG_CHECK_LAUNCH();
+            { LaunchTimer lt(ctx); k_new_of<<<grid, 256, 0, ctx->stream>>>(comm, nv, first.p, newof.p); }
             VG_CHECK_LAUNCH();
         }
         first.release();
@@ -155,20 +188,24 @@ vg_graph *vg_rebuild_new(vg_ctx *ctx, const vg_graph *g, const int32_t *comm) {
         VG_CHECK_LAUNCH();
         { LaunchTimer lt(ctx); k_fill_first<<<grid, 256, 0, ctx->stream>>>(first_pos.p, nv); }
         VG_CHECK_LAUNCH();
-        { LaunchTimer lt(ctx); k_first_ref<<<grid, 256, 0, ctx->stream>>>(comm, nv, g->ref, first_ref.p); }
-        VG_CHECK_LAUNCH();
-        { LaunchTimer lt(ctx); k_first_member<<<grid, 256, 0, ctx->stream>>>(comm, nv, first_pos.p); }
-        VG_CHECK_LAUNCH();
         { LaunchTimer lt(ctx);
-          k_first_flags<<<grid, 256, 0, ctx->stream>>>(comm, nv, g->ref, first_ref.p, first_pos.p,
-                                                       flag_ref.p, flag_pos.p); }
+          k_first_both<<<grid, 256, 0, ctx->stream>>>(comm, nv, g->ref, first_ref.p, first_pos.p); }
         VG_CHECK_LAUNCH();
-        nc = vg_exclusive_scan_i32_to_i64(ctx, flag_ref.p, rank_ref.p, nv);
+        VG_CUDA(cudaMemsetAsync(flag_ref.p, 0, sizeof(int32_t) * nv, ctx->stream));
+        VG_CUDA(cudaMemsetAsync(flag_pos.p, 0, sizeof(int32_t) * nv, ctx->stream));
+        { LaunchTimer lt(ctx);
+          k_comm_flags<<<grid, 256, 0, ctx->stream>>>(first_ref.p, first_pos.p, nv, flag_ref.p,
+                                                      flag_pos.p); }
+        VG_CHECK_LAUNCH();
         vg_scan_i32_async(ctx, flag_pos.p, rank_pos.p, nv, nullptr);
+        nc = vg_exclusive_scan_i32_to_i64(ctx, flag_ref.p, rank_ref.p, nv);
         { LaunchTimer lt(ctx);
-          k_new_ids<<<grid, 256, 0, ctx->stream>>>(comm, nv, first_ref.p, rank_ref.p, first_pos.p,
-                                                   rank_pos.p, new_ref.p, new_pos.p, next_ref.p,
-                                                   next_pos.p); }
+          k_comm_ids<<<grid, 256, 0, ctx->stream>>>(first_ref.p, first_pos.p, nv, rank_ref.p,
+                                                    rank_pos.p, next_ref.p, next_pos.p); }
+        VG_CHECK_LAUNCH();
+        { LaunchTimer lt(ctx);
+          k_vertex_ids<<<grid, 256, 0, ctx->stream>>>(comm, nv, first_ref.p, first_pos.p, new_ref.p,
+                                                      new_pos.p); }
         VG_CHECK_LAUNCH();
     }
     flag_ref.release();
