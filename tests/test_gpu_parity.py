@@ -426,3 +426,12 @@ def test_ba_1m_matches_reference_every_level(ctx, tmp_path, flags):
         cv, _, _ = ctx.louvain_phase(g)
         np.testing.assert_array_equal(cv, ref[0].cvect)
     g.free()
+
+
+def test_edgeless_graph_phase_ends(ctx):
+    """No edges: 2m = 0 makes the modularity NaN; the phase ends after one iteration
+    with every vertex alone."""
+    gref = vo.Graph(np.array([0, 0, 0, 0], np.int64), np.array([], np.int64), np.array([]))
+    cv, mod, it = ctx.louvain_phase(upload(ctx, gref))
+    np.testing.assert_array_equal(cv, np.arange(3))
+    assert it == 1

@@ -1397,7 +1397,7 @@ __global__ void __launch_bounds__(SEG_FINAL) k_mod_seg(const double *__restrict_
                 out[3] = la2;
             } else {
                 bd.iters[j] = bd.iter_dev ? *bd.iter_dev : bd.iter;
-                if (__dsub_rn(m, bd.prev_mod[j]) < bd.thresh[j]) {
+                if (m != m || __dsub_rn(m, bd.prev_mod[j]) < bd.thresh[j]) { // NaN: 2m = 0
                     bd.done[j] = 1;
                     bd.resbuf[j] = (int8_t)bd.past_idx;
                 } else {
@@ -2000,7 +2000,9 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
             }
         }
         currMod = hmod[0];
-        if ((currMod - prevMod) < p->threshold) break;
+        // a NaN modularity (no edges, 2m = 0) would never pass the reference's test
+        // (louvain.cpp:553-563); the phase ends there instead of looping
+        if (std::isnan(currMod) || (currMod - prevMod) < p->threshold) break;
         prevMod = currMod;
         if (prevMod < lower) prevMod = lower;
         if (et == 0) {
