@@ -38,6 +38,15 @@ constexpr int TB = 256;
 #ifndef VG_T32
 #define VG_T32 1
 #endif
+#ifndef VG_T32_GRID
+#define VG_T32_GRID 12 // CTAs per SM in the grid of the degree-<=32 list kernel
+#endif
+#ifndef VG_WS_GRID
+#define VG_WS_GRID 4 // CTAs per SM in the grids of the warp kernels
+#endif
+#ifndef VG_CT_GRID
+#define VG_CT_GRID 2 // CTAs per SM in the grid of the CTA kernel
+#endif
 #ifndef VG_T16_MINB
 #define VG_T16_MINB 3 // resident CTAs per SM of the degree-<=16 list kernel (coloured sweeps)
 #endif
@@ -373,7 +382,7 @@ constexpr int TILE_CAP = 504;          // staged edges per warp (48 KB of shared
 #define VG_TILE_MINB 4 // resident CTAs per SM the register budget is sized for
 #endif
 #ifndef VG_TILE_GRID
-#define VG_TILE_GRID 8 // CTAs per SM in the grid
+#define VG_TILE_GRID 64 // CTAs per SM in the grid (grid-stride; more CTAs balance the tail)
 #endif
 constexpr int TILE_WARPS = VG_TILE_WARPS;
 
@@ -1837,20 +1846,20 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
             k_sweep_thread<true, TMAX, TB><<<vg_grid(ctx, n, TB, 8), TB, 0, ctx->stream>>>(a, list + s, n);
             break;
         case 1:
-            k_sweep_thread<true, 32, 128><<<vg_grid(ctx, n, 128, 12), 128, 0, ctx->stream>>>(a, list + s, n);
+            k_sweep_thread<true, 32, 128><<<vg_grid(ctx, n, 128, VG_T32_GRID), 128, 0, ctx->stream>>>(a, list + s, n);
             break;
         case 2:
-            k_sweep_warp<WS_CAP, WS_WARPS><<<vg_grid(ctx, n * 32, WS_WARPS * 32, 4), WS_WARPS * 32,
+            k_sweep_warp<WS_CAP, WS_WARPS><<<vg_grid(ctx, n * 32, WS_WARPS * 32, VG_WS_GRID), WS_WARPS * 32,
                                              warp_smem_bytes<WS_CAP, WS_WARPS>(), ctx->stream>>>(
                 a, list + s, n);
             break;
         case 3:
-            k_sweep_warp<WT_CAP, WT_WARPS><<<vg_grid(ctx, n * 32, WT_WARPS * 32, 4), WT_WARPS * 32,
+            k_sweep_warp<WT_CAP, WT_WARPS><<<vg_grid(ctx, n * 32, WT_WARPS * 32, VG_WS_GRID), WT_WARPS * 32,
                                              warp_smem_bytes<WT_CAP, WT_WARPS>(), ctx->stream>>>(
                 a, list + s, n);
             break;
         case 4:
-            k_sweep_cta<<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, 2), CT_THREADS, cta_smem_bytes(),
+            k_sweep_cta<<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, VG_CT_GRID), CT_THREADS, cta_smem_bytes(),
                           ctx->stream>>>(a, list + s, n);
             break;
         default:
