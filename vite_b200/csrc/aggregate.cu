@@ -171,6 +171,9 @@ __device__ void bitonic(uint64_t *sk, int n2, int t, int nt) {
 // are then sorted: in registers across the warp when there are at most 32 of
 // them, else in shared memory. A segment with more than H_MAXU distinct keys is
 // flagged for the sorted path.
+#ifndef VG_RH_GRID
+#define VG_RH_GRID 3 // CTAs per SM in the grid of k_rows_hash
+#endif
 constexpr int H_MAXU = 256;
 constexpr int H_CAP = 512;
 constexpr int H_WARPS = 8;
@@ -562,7 +565,7 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     DevBuf<int32_t> flag(ctx, nc);
     if (nc) {
         { LaunchTimer lt(ctx);
-          k_rows_hash<<<vg_grid(ctx, nc * 32, H_WARPS * 32, 3), H_WARPS * 32,
+          k_rows_hash<<<vg_grid(ctx, nc * 32, H_WARPS * 32, VG_RH_GRID), H_WARPS * 32,
                         H_WARPS * sizeof(HashWarpSmem), ctx->stream>>>(
               nc, rstart.p, gk.p, gw.p, uk.p, uw.p, ucount.p, flag.p); }
         VG_CHECK_LAUNCH();

@@ -15,7 +15,7 @@ void vg_throw(vg_status s, const char *fmt, ...) {
 
 int vg_grid(vg_ctx *ctx, int64_t work, int block, int per_sm) {
     int64_t g = (work + block - 1) / block;
-    int64_t cap = (int64_t)ctx->sm_count * per_sm;
+    int64_t cap = (int64_t)ctx->sm_count * per_sm * VG_GRID_SCALE;
     if (g > cap) g = cap;
     if (g < 1) g = 1;
     return (int)g;

@@ -1830,8 +1830,10 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
         if (cls == 0 && natural) {
             if (nv == 0) continue;
             LaunchTimer lt(ctx);
-            k_sweep_tile<TMAX><<<vg_grid(ctx, nv, TILE_WARPS * 32, VG_TILE_GRID), TILE_WARPS * 32, 0,
-                                 ctx->stream>>>(a, nv);
+            const int64_t tiles_blocks = (nv + TILE_WARPS * 32 - 1) / (TILE_WARPS * 32);
+            const int tgrid = (int)std::max<int64_t>(
+                1, std::min<int64_t>(tiles_blocks, (int64_t)VG_TILE_GRID * ctx->sm_count));
+            k_sweep_tile<TMAX><<<tgrid, TILE_WARPS * 32, 0, ctx->stream>>>(a, nv);
             VG_CHECK_LAUNCH();
             continue;
         }

@@ -189,6 +189,11 @@ vg_graph *vg_csr_from_triples(vg_ctx *ctx, int64_t nv, DevBuf<int32_t> &src,
 // ---------------------------------------------------------------------------------
 // kernels shared across files
 
+// grid of at most per_sm * VG_GRID_SCALE blocks per SM for `work` threads in blocks
+// of `block` (grid-stride kernels)
+#ifndef VG_GRID_SCALE
+#define VG_GRID_SCALE 4
+#endif
 int vg_grid(vg_ctx *ctx, int64_t work, int block, int per_sm = 8);
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31; }
