@@ -328,6 +328,7 @@ __global__ void k_big_rowmap(int64_t nc, const int32_t *__restrict__ flag,
 }
 
 constexpr int BIG_CHUNK = 4096;
+constexpr int64_t BIG_RUN_LONG = 1024; // integral weights: longer runs are folded by a warp
 
 // per segment r: its length and chunk count when flagged (more distinct keys than
 // the warp table holds), else 0
@@ -392,12 +393,19 @@ __global__ void k_big_fold(const uint64_t *__restrict__ K, const uint32_t *__res
                            const int64_t *__restrict__ headpos,
                            const int64_t *__restrict__ rowfirst, const int32_t *__restrict__ big_row,
                            const int64_t *__restrict__ rstart, const double *__restrict__ gw,
-                           int32_t *__restrict__ uk, double *__restrict__ uw) {
+                           int32_t *__restrict__ uk, double *__restrict__ uw,
+                           int64_t *__restrict__ long_runs, int64_t long_cap,
+                           unsigned long long *__restrict__ long_count) {
     const uint64_t mask = ((uint64_t)1 << kbits) - 1;
     const int64_t nheads = *nheads_dev;
     for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nheads;
          h += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i0 = headpos[h], i1 = h + 1 < nheads ? headpos[h + 1] : m;
+        if (long_runs && i1 - i0 > BIG_RUN_LONG) { // listed for k_big_fold_long
+            const unsigned long long sl = atomicAdd(long_count, 1ULL);
+            if ((int64_t)sl < long_cap) long_runs[sl] = h;
+            continue;
+        }
         const uint64_t k = K[i0];
         const uint64_t q = k >> kbits;
         double s = gw[V[i0]];
@@ -413,6 +421,47 @@ __global__ void k_big_fold(const uint64_t *__restrict__ K, const uint32_t *__res
         const int64_t o = rstart[big_row[q]] + (h - rowfirst[q]);
         uk[o] = (int32_t)(k & mask);
         uw[o] = s;
+    }
+}
+
+// integral weights only (every partial sum exact, so any order gives the same bits):
+// the listed runs (longer than BIG_RUN_LONG entries), one warp each, eight partial
+// sums per lane
+__global__ void k_big_fold_long(const uint64_t *__restrict__ K, const uint32_t *__restrict__ V,
+                                int64_t m, int kbits, const int64_t *__restrict__ nheads_dev,
+                                const int64_t *__restrict__ headpos,
+                                const int64_t *__restrict__ rowfirst, const int32_t *__restrict__ big_row,
+                                const int64_t *__restrict__ rstart, const double *__restrict__ gw,
+                                int32_t *__restrict__ uk, double *__restrict__ uw,
+                                const int64_t *__restrict__ long_runs, int64_t long_cap,
+                                const unsigned long long *__restrict__ long_count) {
+    const uint64_t mask = ((uint64_t)1 << kbits) - 1;
+    const int64_t nheads = *nheads_dev;
+    const int64_t nl = min((int64_t)*long_count, long_cap);
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < nl; r += nw) {
+        const int64_t h = long_runs[r];
+        const int64_t i0 = headpos[h], i1 = h + 1 < nheads ? headpos[h + 1] : m;
+        double ps[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int64_t j = i0 + lane;
+        for (; j + 7 * 32 < i1; j += 8 * 32) {
+#pragma unroll
+            for (int t = 0; t < 8; t++) ps[t] = __dadd_rn(ps[t], gw[V[j + t * 32]]);
+        }
+        for (; j < i1; j += 32) ps[0] = __dadd_rn(ps[0], gw[V[j]]);
+#pragma unroll
+        for (int t = 1; t < 8; t++) ps[0] = __dadd_rn(ps[0], ps[t]);
+        double sum = ps[0];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum = __dadd_rn(sum, __shfl_xor_sync(0xffffffffu, sum, o));
+        if (lane == 0) {
+            const uint64_t k = K[i0];
+            const uint64_t q = k >> kbits;
+            const int64_t o = rstart[big_row[q]] + (h - rowfirst[q]);
+            uk[o] = (int32_t)(k & mask);
+            uw[o] = sum;
+        }
     }
 }
 
@@ -499,6 +548,7 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
                             const int32_t *new_row, const int32_t *new_key, int64_t nc,
                             const int32_t *key_to_pos) {
     const int64_t nv = g->nv, ne = g->ne;
+    const int integral = g->integral == 1 ? 1 : 0; // every weight a small integer
     static bool configured = false;
     if (!configured) {
         VG_CUDA(cudaFuncSetAttribute(k_rows_hash, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -616,10 +666,23 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
                                                                             rowfirst.p, headpos.p); }
             VG_CHECK_LAUNCH();
             hr.release();
+            // integral weights: runs longer than BIG_RUN_LONG are listed for a warp each
+            const int64_t lcap = integral ? m / (BIG_RUN_LONG + 1) + 1 : 0;
+            DevBuf<int64_t> lruns(ctx, lcap);
+            DevBuf<unsigned long long> lcount(ctx, integral ? 1 : 0);
+            if (integral)
+                VG_CUDA(cudaMemsetAsync(lcount.p, 0, sizeof(unsigned long long), ctx->stream));
             { LaunchTimer lt(ctx);
               k_big_fold<<<vg_grid(ctx, m, 128), 128, 0, ctx->stream>>>(
                   K.p, V.p, m, kbits, tot.p + 3, headpos.p, rowfirst.p, big_row.p, rstart.p, gw.p,
-                  uk.p, uw.p); }
+                  uk.p, uw.p, lruns.p, lcap, lcount.p); }
+            VG_CHECK_LAUNCH();
+            if (integral) {
+                LaunchTimer lt(ctx);
+                k_big_fold_long<<<vg_grid(ctx, lcap * 32, 256), 256, 0, ctx->stream>>>(
+                    K.p, V.p, m, kbits, tot.p + 3, headpos.p, rowfirst.p, big_row.p, rstart.p, gw.p,
+                    uk.p, uw.p, lruns.p, lcap, lcount.p);
+            }
             VG_CHECK_LAUNCH();
             { LaunchTimer lt(ctx);
               k_big_counts<<<vg_grid(ctx, nbig, 256), 256, 0, ctx->stream>>>(

@@ -1197,7 +1197,18 @@ __global__ void k_degree_long(const int64_t *__restrict__ rowptr, const double *
         const int64_t E0 = rowptr[v], E1 = rowptr[v + 1];
         double sum = 0.0;
         if (integral) {
-            for (int64_t k = E0 + lane; k < E1; k += 32) sum = __dadd_rn(sum, w[k]);
+            // eight independent partial sums per lane (exact in any order), so eight
+            // loads are in flight instead of one chain
+            double ps[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            int64_t k = E0 + lane;
+            for (; k + 7 * 32 < E1; k += 8 * 32) {
+#pragma unroll
+                for (int t = 0; t < 8; t++) ps[t] = __dadd_rn(ps[t], w[k + t * 32]);
+            }
+            for (; k < E1; k += 32) ps[0] = __dadd_rn(ps[0], w[k]);
+#pragma unroll
+            for (int t = 1; t < 8; t++) ps[0] = __dadd_rn(ps[0], ps[t]);
+            sum = ps[0];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) sum = __dadd_rn(sum, __shfl_xor_sync(full, sum, o));
         } else {
