@@ -200,6 +200,47 @@ __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
     for (int64_t row = wg; row < nc; row += nw) {
         const int64_t b = rstart[row];
         const int64_t L = rstart[row + 1] - b;
+        if (L <= 32) {
+            // one chunk: the leader of each key folds its lanes in lane order (the
+            // table path's sum for a key first met in this chunk), and the leaders'
+            // (key, sum) pairs are sorted across the lanes; no table needed
+            const bool has = lane < L;
+            const int32_t k = has ? gk[b + lane] : -2 - lane;
+            const double w = has ? gw[b + lane] : 0.0;
+            S.stage[lane] = w;
+            const unsigned peers = __match_any_sync(full, k);
+            __syncwarp();
+            const bool lead = has && lane == __ffs(peers) - 1;
+            double val = w;
+            const unsigned above = peers & ~((2u << lane) - 1u);
+            if (lead && above) val = vg_fold_above(val, S.stage, above);
+            const int U = __popc(__ballot_sync(full, lead));
+            int32_t key = lead ? k : INT_MAX;
+#pragma unroll
+            for (int k2 = 2; k2 <= 32; k2 <<= 1)
+#pragma unroll
+                for (int j = k2 >> 1; j > 0; j >>= 1) {
+                    const int32_t pk = __shfl_xor_sync(full, key, j);
+                    const double pv = __shfl_xor_sync(full, val, j);
+                    const bool up = (lane & k2) == 0;
+                    const bool low = (lane & j) == 0;
+                    const bool take = (low == up) ? (pk < key) : (pk > key);
+                    if (take) {
+                        key = pk;
+                        val = pv;
+                    }
+                }
+            if (lane < U) {
+                uk[b + lane] = key;
+                uw[b + lane] = val;
+            }
+            if (lane == 0) {
+                ucount[row] = U;
+                flag[row] = 0;
+            }
+            __syncwarp();
+            continue;
+        }
         int logcap = 5;
         while ((1 << logcap) < 2 * L && (1 << logcap) < H_CAP) logcap++;
         const int cap = 1 << logcap; // > twice the distinct keys held (at most H_MAXU + 31)
