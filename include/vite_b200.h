@@ -155,6 +155,39 @@ vg_status vg_vertex_degree_noalloc(int64_t nv, const int64_t *d_rowptr, const do
 
 /* --- the Louvain path ----------------------------------------------------------- */
 
+/* Launch tuning of the local-moving sweep, held per context. It has no counterpart
+ * in the reference (its sweep is one loop per rank); it chooses which kernel
+ * handles a vertex of degree d: d <= 16 one thread; d <= 32 one thread when t32 is
+ * 1 (else the small warp table); d <= ws_max one warp with a 256-slot table;
+ * d <= wt_max one warp with a 1024-slot table; d <= ct_max one CTA with an 8192-slot
+ * table; above, the hub path (many CTAs per row). tile_grid is the number of CTAs
+ * per SM of the degree <= 16 sweep in vertex order. Every class folds a vertex's
+ * counters in CSR order except the two CTA-based ones, whose slices meet through
+ * FP64 atomics: with unit or integral weights any setting gives the same bits, with
+ * real weights results agree to the last few bits. */
+typedef struct vg_tuning {
+    int32_t t32;       /* 0 or 1 */
+    int32_t ws_max;    /* 32..128 */
+    int32_t wt_max;    /* ws_max..512 */
+    int32_t ct_max;    /* wt_max..4096 */
+    int32_t tile_grid; /* 1..1024 */
+} vg_tuning;
+
+/* The context's current tuning (the built-in defaults until set). */
+vg_status vg_ctx_get_tuning(const vg_ctx *ctx, vg_tuning *out);
+/* Set the tuning; VG_ERR_ARG when a field is outside its range above. */
+vg_status vg_ctx_set_tuning(vg_ctx *ctx, const vg_tuning *t);
+
+/* The autotuner (no counterpart in the reference). Starting from the context's
+ * tuning, it varies one field at a time over a few candidate values and keeps a
+ * change when it lowers the summed sweep time of the first `sweeps` iterations (1..8;
+ * 0 means 2) of a plain phase on every graph given, each timed twice, the faster
+ * taken. The graphs are left as they were (each trial runs on a shallow copy). The
+ * best tuning is set on the context and returned with its summed sweep time and that
+ * of the tuning it started from (milliseconds; either pointer may be NULL). */
+vg_status vg_autotune(vg_ctx *ctx, vg_graph *const *graphs, int32_t n, int32_t sweeps,
+                      vg_tuning *best_out, double *best_ms_out, double *start_ms_out);
+
 /* One Louvain phase: distLouvainMethod / ...WithColoring / ...VertexOrder
  * (louvain.cpp:7-1938). Returns the phase's modularity (`prevMod` of the
  * reference), its iteration count and, if cvect_out is not NULL, the community

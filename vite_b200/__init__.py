@@ -37,6 +37,7 @@ EXPORTED_SYMBOLS = [
     "vg_graph_reorder", "vg_vertex_degree_noalloc",
     "vg_batch_create", "vg_batch_destroy", "vg_batch_submit", "vg_batch_step", "vg_batch_poll",
     "vg_batch_result", "vg_batch_forget", "vg_batch_get_stats", "vg_compare_communities",
+    "vg_ctx_get_tuning", "vg_ctx_set_tuning", "vg_autotune",
 ]
 
 VG_BATCH_TAKE = 1
@@ -78,6 +79,15 @@ class CompareStats(C.Structure):
                 ("same_same", C.c_int64), ("same_diff", C.c_int64), ("diff_same", C.c_int64),
                 ("precision", C.c_double), ("recall", C.c_double), ("fscore", C.c_double),
                 ("gini1", C.c_double), ("gini2", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Tuning(C.Structure):
+    """vg_tuning: which sweep kernel takes each degree, and the tile grid."""
+    _fields_ = [("t32", C.c_int32), ("ws_max", C.c_int32), ("wt_max", C.c_int32),
+                ("ct_max", C.c_int32), ("tile_grid", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -149,6 +159,10 @@ def lib() -> C.CDLL:
         L.vg_batch_forget.argtypes = [vp, C.c_int64]
         L.vg_batch_get_stats.argtypes = [vp, C.POINTER(BatchStats)]
         L.vg_compare_communities.argtypes = [vp, C.c_int64, _i64p, _i64p, C.POINTER(CompareStats)]
+        L.vg_ctx_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.vg_ctx_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.vg_autotune.argtypes = [vp, C.POINTER(vp), C.c_int32, C.c_int32, C.POINTER(Tuning),
+                                  _f64p, _f64p]
         for name in EXPORTED_SYMBOLS:
             if name not in ("vg_last_error", "vg_ctx_bytes_in_use"):
                 getattr(L, name).restype = C.c_int
@@ -380,6 +394,28 @@ class Context:
         self._check(lib().vg_compare_communities(self.handle, len(a), _ptr(a), _ptr(b),
                                                  C.byref(st)))
         return st.as_dict()
+
+    @property
+    def tuning(self) -> dict:
+        """The sweep launch tuning in use (vg_ctx_get_tuning)."""
+        t = Tuning()
+        self._check(lib().vg_ctx_get_tuning(self.handle, C.byref(t)))
+        return t.as_dict()
+
+    @tuning.setter
+    def tuning(self, value: dict) -> None:
+        t = Tuning(**{**self.tuning, **value})
+        self._check(lib().vg_ctx_set_tuning(self.handle, C.byref(t)))
+
+    def autotune(self, graphs: list, sweeps: int = 2) -> dict:
+        """vg_autotune over `graphs`: sets and returns the fastest tuning found, with the
+        summed sweep times (ms) of it and of the tuning it started from."""
+        arr = (C.c_void_p * len(graphs))(*[g.handle for g in graphs])
+        t = Tuning()
+        best, start = C.c_double(), C.c_double()
+        self._check(lib().vg_autotune(self.handle, arr, len(graphs), sweeps, C.byref(t),
+                                      C.byref(best), C.byref(start)))
+        return {"tuning": t.as_dict(), "sweep_ms": best.value, "start_sweep_ms": start.value}
 
     def batch(self, budget: int = 0) -> "Batch":
         return Batch(self, budget)

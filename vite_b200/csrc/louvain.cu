@@ -65,12 +65,18 @@ constexpr int CT_CAP = 8192;
 constexpr int CT_THREADS = 256;
 constexpr int32_t EMPTY = -1;
 
-__host__ __device__ __forceinline__ int degree_class(int64_t d) {
+// the degree bounds of classes 1-4 (the context's vg_tuning, checked against the
+// table capacities above)
+struct ClassBounds {
+    int32_t t32, ws, wt, ct;
+};
+
+__host__ __device__ __forceinline__ int degree_class(int64_t d, const ClassBounds &b) {
     if (d <= TMAX) return 0;
-    if (VG_T32 && d <= 32) return 1;
-    if (d <= WS_MAXDEG) return 2;
-    if (d <= WT_MAXDEG) return 3;
-    if (d <= CT_MAXDEG) return 4;
+    if (b.t32 && d <= 32) return 1;
+    if (d <= b.ws) return 2;
+    if (d <= b.wt) return 3;
+    if (d <= b.ct) return 4;
     return 5;
 }
 
@@ -1546,26 +1552,26 @@ __global__ void k_narrow(const int64_t *__restrict__ in, int64_t n, int64_t lim,
 // bucket key of a vertex: (color bucket, degree class)
 __device__ __forceinline__ int32_t bucket_key(const int64_t *__restrict__ rowptr, int64_t i,
                                               const int32_t *__restrict__ colors, int64_t numColor,
-                                              int64_t *d_out) {
+                                              int64_t *d_out, const ClassBounds &bnd) {
     const int64_t d = rowptr[i + 1] - rowptr[i];
     int64_t cb = 0;
     if (colors) cb = colors[i] < 0 ? numColor - 1 : colors[i];
     *d_out = d;
-    return (int32_t)(cb * NCLS + degree_class(d));
+    return (int32_t)(cb * NCLS + degree_class(d, bnd));
 }
 
 // Each block histograms a contiguous chunk of vertices in shared memory and
 // adds its counts to the global ones (one atomic per bucket per block).
 __global__ void k_bucket_count(const int64_t *__restrict__ rowptr, int64_t nv,
                                const int32_t *__restrict__ colors, int64_t numColor, int nb,
-                               int64_t chunk, int32_t *__restrict__ counts) {
+                               int64_t chunk, int32_t *__restrict__ counts, ClassBounds bnd) {
     extern __shared__ int32_t sc[];
     for (int k = threadIdx.x; k < nb; k += blockDim.x) sc[k] = 0;
     __syncthreads();
     const int64_t b0 = blockIdx.x * chunk, b1 = min(nv, b0 + chunk);
     for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
         int64_t d;
-        atomicAdd(&sc[bucket_key(rowptr, i, colors, numColor, &d)], 1);
+        atomicAdd(&sc[bucket_key(rowptr, i, colors, numColor, &d, bnd)], 1);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < nb; k += blockDim.x)
@@ -1582,7 +1588,7 @@ constexpr int PLACE_THREADS = 256;
 
 __global__ void __launch_bounds__(PLACE_THREADS) k_bucket_place_ordered(
     const int64_t *__restrict__ rowptr, int64_t nv, int nb, int64_t chunk,
-    int32_t *__restrict__ fill, int32_t *__restrict__ list) {
+    int32_t *__restrict__ fill, int32_t *__restrict__ list, ClassBounds bnd) {
     __shared__ int32_t cnt[PLACE_THREADS / 32][32];
     __shared__ int32_t base[32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1593,14 +1599,14 @@ __global__ void __launch_bounds__(PLACE_THREADS) k_bucket_place_ordered(
     const int64_t b0 = blockIdx.x * chunk, b1 = min(nv, b0 + chunk);
     int64_t d;
     for (int64_t i = b0 + threadIdx.x; i < b1; i += PLACE_THREADS)
-        atomicAdd(&base[bucket_key(rowptr, i, nullptr, 1, &d)], 1);
+        atomicAdd(&base[bucket_key(rowptr, i, nullptr, 1, &d, bnd)], 1);
     __syncthreads();
     if (threadIdx.x < nb) base[threadIdx.x] = base[threadIdx.x] ? atomicAdd(&fill[threadIdx.x], base[threadIdx.x]) : 0;
     __syncthreads();
     for (int64_t r0 = b0; r0 < b1; r0 += PLACE_THREADS) {
         const int64_t i = r0 + threadIdx.x;
         const bool valid = i < b1;
-        const int k = valid ? bucket_key(rowptr, i, nullptr, 1, &d) : 32 + lane;
+        const int k = valid ? bucket_key(rowptr, i, nullptr, 1, &d, bnd) : 32 + lane;
         const unsigned peers = __match_any_sync(0xffffffffu, k);
         if (lane < 32) cnt[warp][lane] = 0;
         __syncwarp();
@@ -1623,7 +1629,7 @@ __global__ void __launch_bounds__(PLACE_THREADS) k_bucket_place_ordered(
 __global__ void k_bucket_place(const int64_t *__restrict__ rowptr, int64_t nv,
                                const int32_t *__restrict__ colors, int64_t numColor, int nb,
                                int64_t chunk, int32_t *__restrict__ fill,
-                               int32_t *__restrict__ list) {
+                               int32_t *__restrict__ list, ClassBounds bnd) {
     extern __shared__ int32_t sc[]; // [0, nb) counts then local cursors, [nb, 2nb) bases
     int32_t *base = sc + nb;
     for (int k = threadIdx.x; k < nb; k += blockDim.x) sc[k] = 0;
@@ -1631,7 +1637,7 @@ __global__ void k_bucket_place(const int64_t *__restrict__ rowptr, int64_t nv,
     const int64_t b0 = blockIdx.x * chunk, b1 = min(nv, b0 + chunk);
     int64_t d;
     for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x)
-        atomicAdd(&sc[bucket_key(rowptr, i, colors, numColor, &d)], 1);
+        atomicAdd(&sc[bucket_key(rowptr, i, colors, numColor, &d, bnd)], 1);
     __syncthreads();
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
         base[k] = sc[k] ? atomicAdd(&fill[k], sc[k]) : 0;
@@ -1639,7 +1645,7 @@ __global__ void k_bucket_place(const int64_t *__restrict__ rowptr, int64_t nv,
     }
     __syncthreads();
     for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-        const int32_t k = bucket_key(rowptr, i, colors, numColor, &d);
+        const int32_t k = bucket_key(rowptr, i, colors, numColor, &d, bnd);
         list[base[k] + atomicAdd(&sc[k], 1)] = (int32_t)i;
     }
 }
@@ -1648,6 +1654,30 @@ __global__ void k_bucket_place(const int64_t *__restrict__ rowptr, int64_t nv,
 
 // ---------------------------------------------------------------------------------
 // host side
+
+// the context's tuning with unset (zero) fields at the built-in defaults
+static vg_tuning effective_tuning(const vg_ctx *ctx) {
+    vg_tuning t = ctx->tune;
+    if (t.ws_max == 0) {
+        t.t32 = VG_T32;
+        t.ws_max = WS_MAXDEG;
+        t.wt_max = WT_MAXDEG;
+        t.ct_max = CT_MAXDEG;
+    }
+    if (t.tile_grid == 0) t.tile_grid = VG_TILE_GRID;
+    return t;
+}
+
+static bool tuning_valid(const vg_tuning &t) {
+    return (t.t32 == 0 || t.t32 == 1) && t.ws_max >= 32 && t.ws_max <= WS_CAP / 2 &&
+           t.wt_max >= t.ws_max && t.wt_max <= WT_CAP / 2 && t.ct_max >= t.wt_max &&
+           t.ct_max <= CT_CAP / 2 && t.tile_grid >= 1 && t.tile_grid <= 1024;
+}
+
+static ClassBounds class_bounds(const vg_ctx *ctx) {
+    const vg_tuning t = effective_tuning(ctx);
+    return ClassBounds{t.t32, t.ws_max, t.wt_max, t.ct_max};
+}
 
 struct Buckets {
     DevBuf<int32_t> list;
@@ -1659,6 +1689,7 @@ static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors,
                           Buckets &b) {
     const int64_t nv = g->nv;
     const int64_t nb = numColor * NCLS;
+    const ClassBounds bnd = class_bounds(ctx);
     VG_REQUIRE(nb <= 6000, "too many color buckets (%lld colors)", (long long)numColor);
     b.ncolor = numColor;
     DevBuf<int32_t> counts(ctx, nb);
@@ -1668,7 +1699,7 @@ static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors,
     if (nv) {
         LaunchTimer lt(ctx);
         k_bucket_count<<<blocks, 256, sizeof(int32_t) * nb, ctx->stream>>>(
-            g->rowptr, nv, colors, numColor, (int)nb, chunk, counts.p);
+            g->rowptr, nv, colors, numColor, (int)nb, chunk, counts.p, bnd);
     }
     VG_CHECK_LAUNCH();
     std::vector<int32_t> hc(nb);
@@ -1686,12 +1717,12 @@ static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors,
     b.list.alloc(ctx, nv);
     if (nv && !colors && nb <= 32) {
         LaunchTimer lt(ctx);
-        k_bucket_place_ordered<<<blocks, PLACE_THREADS, 0, ctx->stream>>>(g->rowptr, nv, (int)nb,
-                                                                          chunk, counts.p, b.list.p);
+        k_bucket_place_ordered<<<blocks, PLACE_THREADS, 0, ctx->stream>>>(
+            g->rowptr, nv, (int)nb, chunk, counts.p, b.list.p, bnd);
     } else if (nv) {
         LaunchTimer lt(ctx);
         k_bucket_place<<<blocks, 256, 2 * sizeof(int32_t) * nb, ctx->stream>>>(
-            g->rowptr, nv, colors, numColor, (int)nb, chunk, counts.p, b.list.p);
+            g->rowptr, nv, colors, numColor, (int)nb, chunk, counts.p, b.list.p, bnd);
     }
     VG_CHECK_LAUNCH();
     vg_sync(ctx); // keep `fill` alive until the copy is done
@@ -1843,7 +1874,8 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
             LaunchTimer lt(ctx);
             const int64_t tiles_blocks = (nv + TILE_WARPS * 32 - 1) / (TILE_WARPS * 32);
             const int tgrid = (int)std::max<int64_t>(
-                1, std::min<int64_t>(tiles_blocks, (int64_t)VG_TILE_GRID * ctx->sm_count));
+                1, std::min<int64_t>(tiles_blocks,
+                                     (int64_t)effective_tuning(ctx).tile_grid * ctx->sm_count));
             k_sweep_tile<TMAX><<<tgrid, TILE_WARPS * 32, 0, ctx->stream>>>(a, nv);
             VG_CHECK_LAUNCH();
             continue;
@@ -1888,8 +1920,9 @@ struct PhaseTiming {
 };
 
 // the phase proper; returns the communities in g->comm
+// max_iters > 0 stops after that many iterations (the autotuner's timing runs)
 static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double *mod_out,
-                      int32_t *iters_out, PhaseTiming *timing) {
+                      int32_t *iters_out, PhaseTiming *timing, int max_iters = 0) {
     configure_kernels_once();
     const int64_t nv = g->nv;
     int ordering = p->ordering;
@@ -2015,6 +2048,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
             timing->sweep_ms += ms;
             timing->edges += g->ne;
         }
+        if (max_iters > 0 && numIters >= max_iters) break;
         if (et == 3 || et == 4) { // ETLocalOrRemote == false (louvain.cpp:112-121)
             if ((long)hmod[1] >= 90) { // ET_CUTOFF (louvain.hpp:70)
                 currMod = -1;
@@ -2309,6 +2343,100 @@ extern "C" vg_status vg_louvain_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_p
         VG_CUDA(cudaSetDevice(ctx->device));
         run_phase(ctx, g, p, mod_out, iters_out, nullptr);
         if (cvect_out) vg_download_comm_ref(ctx, g, g->comm, cvect_out);
+    });
+}
+
+extern "C" vg_status vg_ctx_get_tuning(const vg_ctx *ctx, vg_tuning *out) {
+    if (!ctx || !out) return VG_ERR_ARG;
+    *out = effective_tuning(ctx);
+    return VG_OK;
+}
+
+extern "C" vg_status vg_ctx_set_tuning(vg_ctx *ctx, const vg_tuning *t) {
+    if (!ctx || !t) return VG_ERR_ARG;
+    if (!tuning_valid(*t)) {
+        ctx->last_error = "vg_ctx_set_tuning: t32 must be 0 or 1, 32 <= ws_max <= wt_max <= ct_max "
+                          "with ws_max <= 128, wt_max <= 512, ct_max <= 4096, 1 <= tile_grid <= 1024";
+        return VG_ERR_ARG;
+    }
+    ctx->tune = *t;
+    return VG_OK;
+}
+
+// Coordinate descent over the tuning fields: each candidate's cost is the summed
+// sweep time (CUDA events around the sweep launches) of the first `sweeps`
+// iterations of a plain phase on every graph, the faster of two timings. A change
+// is kept when it saves more than 1 %.
+extern "C" vg_status vg_autotune(vg_ctx *ctx, vg_graph *const *graphs, int32_t n, int32_t sweeps,
+                                 vg_tuning *best_out, double *best_ms_out, double *start_ms_out) {
+    if (!ctx || !graphs || n < 1 || sweeps < 0 || sweeps > 8) return VG_ERR_ARG;
+    for (int32_t i = 0; i < n; i++)
+        if (!graphs[i]) return VG_ERR_ARG;
+    const vg_tuning start = effective_tuning(ctx);
+    return vg_guard(ctx, [&] {
+        VG_CUDA(cudaSetDevice(ctx->device));
+        const int its = sweeps == 0 ? 2 : sweeps;
+        vg_phase_params pp{};
+        pp.lower = -1.0;
+        pp.threshold = 1e-6;
+        pp.et_type = 0;
+        pp.et_delta = 1.0;
+        pp.ordering = 0;
+        auto one = [&](const vg_tuning &t) {
+            ctx->tune = t;
+            double total = 0.0;
+            for (int32_t i = 0; i < n; i++) {
+                vg_graph tmp = *graphs[i]; // shares the CSR; the trial's communities are its own
+                tmp.comm = nullptr;
+                PhaseTiming pt;
+                double mod = 0.0;
+                int32_t it = 0;
+                try {
+                    run_phase(ctx, &tmp, &pp, &mod, &it, &pt, its);
+                } catch (...) {
+                    if (tmp.comm) vg_free(ctx, tmp.comm, sizeof(int32_t) * tmp.nv);
+                    throw;
+                }
+                if (tmp.comm) vg_free(ctx, tmp.comm, sizeof(int32_t) * tmp.nv);
+                graphs[i]->integral = tmp.integral; // the cached weight test
+                total += pt.sweep_ms;
+            }
+            return total;
+        };
+        auto cost = [&](const vg_tuning &t) { return std::min(one(t), one(t)); };
+        vg_tuning best = start;
+        double best_ms = 0.0, start_ms = 0.0;
+        try {
+            start_ms = best_ms = cost(start);
+            const int32_t t32s[] = {1, 0};
+            const int32_t wss[] = {64, 96, 128};
+            const int32_t wts[] = {256, 384, 512};
+            const int32_t cts[] = {1024, 2048, 4096};
+            const int32_t grids[] = {16, 32, 64, 128};
+            auto consider = [&](vg_tuning t) {
+                if (!tuning_valid(t)) return;
+                if (t.t32 == best.t32 && t.ws_max == best.ws_max && t.wt_max == best.wt_max &&
+                    t.ct_max == best.ct_max && t.tile_grid == best.tile_grid)
+                    return;
+                const double c = cost(t);
+                if (c < 0.99 * best_ms) {
+                    best = t;
+                    best_ms = c;
+                }
+            };
+            for (int32_t v : t32s) { vg_tuning t = best; t.t32 = v; consider(t); }
+            for (int32_t v : wss) { vg_tuning t = best; t.ws_max = v; consider(t); }
+            for (int32_t v : wts) { vg_tuning t = best; t.wt_max = v; consider(t); }
+            for (int32_t v : cts) { vg_tuning t = best; t.ct_max = v; consider(t); }
+            for (int32_t v : grids) { vg_tuning t = best; t.tile_grid = v; consider(t); }
+        } catch (...) {
+            ctx->tune = start;
+            throw;
+        }
+        ctx->tune = best;
+        if (best_out) *best_out = best;
+        if (best_ms_out) *best_ms_out = best_ms;
+        if (start_ms_out) *start_ms_out = start_ms;
     });
 }
 

@@ -57,6 +57,8 @@ struct vg_ctx {
     int64_t profile_launches = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> event_pool;
+    // sweep launch tuning (vg_ctx_set_tuning / vg_autotune); all zero = built-in defaults
+    vg_tuning tune{};
 };
 
 // stream-ordered device allocation accounted against the context budget
