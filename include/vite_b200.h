@@ -122,6 +122,17 @@ vg_status vg_graph_info(const vg_graph *g, int64_t *nv, int64_t *ne);
 vg_status vg_graph_download(vg_ctx *ctx, const vg_graph *g, int64_t *rowptr, vg_edge *edges);
 vg_status vg_graph_free(vg_ctx *ctx, vg_graph *g);
 
+/* Vite's binary graph file ([nv][ne][rowptr x (nv+1)][Edge x ne], all little-endian
+ * int64 / f64; read by loadDistGraphMPIIO, distgraph.cpp:119-253, written by writeGraph
+ * and the converters, converters/convert.cpp:245-278) straight to and from a device
+ * graph. The reader streams the file through pinned host buffers with the copies and
+ * the conversion overlapping the reads, rebases the offsets to start at zero
+ * (distgraph.cpp:244-247) and rejects a truncated file, offsets that decrease or do
+ * not end at ne, and tails outside [0, nv) with VG_ERR_ARG. The writer writes the
+ * graph in reference vertex order, as vg_graph_download returns it. */
+vg_status vg_graph_read_vite(vg_ctx *ctx, const char *path, vg_graph **out);
+vg_status vg_graph_write_vite(vg_ctx *ctx, const vg_graph *g, const char *path);
+
 /* Store the graph in another vertex order on the device (no reference
  * counterpart: the reference keeps its input order). mode 1: locality order
  * (multi-source BFS clusters) so that a sweep's gathers stay in few cache

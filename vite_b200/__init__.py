@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = [
     "vg_batch_create", "vg_batch_destroy", "vg_batch_submit", "vg_batch_step", "vg_batch_poll",
     "vg_batch_result", "vg_batch_forget", "vg_batch_get_stats", "vg_compare_communities",
     "vg_ctx_get_tuning", "vg_ctx_set_tuning", "vg_autotune",
+    "vg_graph_read_vite", "vg_graph_write_vite",
 ]
 
 VG_BATCH_TAKE = 1
@@ -159,6 +160,8 @@ def lib() -> C.CDLL:
         L.vg_batch_forget.argtypes = [vp, C.c_int64]
         L.vg_batch_get_stats.argtypes = [vp, C.POINTER(BatchStats)]
         L.vg_compare_communities.argtypes = [vp, C.c_int64, _i64p, _i64p, C.POINTER(CompareStats)]
+        L.vg_graph_read_vite.argtypes = [vp, C.c_char_p, C.POINTER(vp)]
+        L.vg_graph_write_vite.argtypes = [vp, vp, C.c_char_p]
         L.vg_ctx_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.vg_ctx_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.vg_autotune.argtypes = [vp, C.POINTER(vp), C.c_int32, C.c_int32, C.POINTER(Tuning),
@@ -394,6 +397,16 @@ class Context:
         self._check(lib().vg_compare_communities(self.handle, len(a), _ptr(a), _ptr(b),
                                                  C.byref(st)))
         return st.as_dict()
+
+    def read_vite(self, path: str) -> Graph:
+        """A Vite binary graph file straight into a device graph (vg_graph_read_vite)."""
+        h = C.c_void_p()
+        self._check(lib().vg_graph_read_vite(self.handle, os.fsencode(path), C.byref(h)))
+        return Graph(self, h)
+
+    def write_vite(self, g: Graph, path: str) -> None:
+        """Write g as a Vite binary graph file, reference vertex order (vg_graph_write_vite)."""
+        self._check(lib().vg_graph_write_vite(self.handle, g.handle, os.fsencode(path)))
 
     @property
     def tuning(self) -> dict:
