@@ -19,7 +19,7 @@
 
 namespace {
 
-constexpr size_t IO_CHUNK = 64ull << 20; // bytes per pinned buffer (a multiple of 16)
+constexpr size_t IO_CHUNK = 64ull << 20; // most bytes per pinned buffer (a multiple of 16)
 
 // flags row offsets (n1 of them, first = base) that decrease or do not end at base + ne
 __global__ void k_check_offsets(const int64_t *__restrict__ rp, int64_t n1, int64_t base,
@@ -119,9 +119,13 @@ extern "C" vg_status vg_graph_read_vite(vg_ctx *ctx, const char *path, vg_graph 
         DevBuf<double> w(ctx, ne);
         DevBuf<int> bad(ctx, 2);
         VG_CUDA(cudaMemsetAsync(bad.p, 0, 2 * sizeof(int), ctx->stream));
+        // pinned buffers sized to the file (a small file needs no 64 MiB buffers), a
+        // multiple of 16 bytes so edge records never straddle two chunks
+        const size_t chunk = (size_t)std::min<int64_t>(
+            (int64_t)IO_CHUNK, (std::max<int64_t>(std::max(rp_bytes, e_bytes), 4096) + 15) & ~15LL);
         Pinned hb[2];
-        VG_CUDA(cudaMallocHost(&hb[0].p, IO_CHUNK));
-        VG_CUDA(cudaMallocHost(&hb[1].p, IO_CHUNK));
+        VG_CUDA(cudaMallocHost(&hb[0].p, chunk));
+        VG_CUDA(cudaMallocHost(&hb[1].p, chunk));
         cudaEvent_t done[2] = {nullptr, nullptr};
         VG_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
         VG_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
@@ -139,9 +143,9 @@ extern "C" vg_status vg_graph_read_vite(vg_ctx *ctx, const char *path, vg_graph 
             // row offsets
             int64_t base = 0;
             int k = 0;
-            for (int64_t off = 0; off < rp_bytes; off += IO_CHUNK, k++) {
+            for (int64_t off = 0; off < rp_bytes; off += (int64_t)chunk, k++) {
                 const int b = k & 1;
-                const size_t len = (size_t)std::min<int64_t>(IO_CHUNK, rp_bytes - off);
+                const size_t len = (size_t)std::min<int64_t>((int64_t)chunk, rp_bytes - off);
                 take(b);
                 pread_all(f.fd, hb[b].p, len, 16 + off, path);
                 if (off == 0) base = *static_cast<int64_t *>(hb[b].p);
@@ -162,7 +166,7 @@ extern "C" vg_status vg_graph_read_vite(vg_ctx *ctx, const char *path, vg_graph 
             VG_CHECK_LAUNCH();
             // edge records, chunk by chunk through two device staging buffers
             if (ne) {
-                const int64_t per = (int64_t)(IO_CHUNK / 16);
+                const int64_t per = (int64_t)(chunk / 16);
                 DevBuf<longlong2> stage[2];
                 stage[0].alloc(ctx, (size_t)std::min<int64_t>(per, ne));
                 stage[1].alloc(ctx, (size_t)std::min<int64_t>(per, ne));
