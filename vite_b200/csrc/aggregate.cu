@@ -387,7 +387,9 @@ __global__ void k_big_prep(int64_t nc, const int32_t *__restrict__ flag,
 // one block per chunk of BIG_CHUNK entries of a flagged segment; cb: exclusive
 // prefix of the chunk counts over all nc segments (unflagged ones hold none, so the
 // largest r with cb[r] <= c owns chunk c); q = bigidx[r] is the segment's rank
-// among the flagged ones and leads its sort key
+// among the flagged ones and leads its sort key; the payload is the entry's index
+// inside its segment (the folds add the segment's start back), so a level of 2^32
+// or more entries still fits the 32-bit payload
 __global__ void k_big_keys(int64_t nc, const int64_t *__restrict__ cb, int64_t nchunks,
                            const int64_t *__restrict__ bigidx, const int64_t *__restrict__ rstart,
                            const int64_t *__restrict__ boff, const int32_t *__restrict__ gk,
@@ -404,7 +406,7 @@ __global__ void k_big_keys(int64_t nc, const int64_t *__restrict__ cb, int64_t n
         const int64_t i0 = (c - cb[r]) * BIG_CHUNK, i1 = min(i0 + BIG_CHUNK, L);
         for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
             K[o + i] = ((uint64_t)q << kbits) | (uint64_t)(uint32_t)gk[b + i];
-            V[o + i] = (uint32_t)(b + i);
+            V[o + i] = (uint32_t)i;
         }
     }
 }
@@ -449,17 +451,19 @@ __global__ void k_big_fold(const uint64_t *__restrict__ K, const uint32_t *__res
         }
         const uint64_t k = K[i0];
         const uint64_t q = k >> kbits;
-        double s = gw[V[i0]];
+        const int64_t seg = rstart[big_row[q]];
+        const double *__restrict__ sw = gw + seg; // the segment's weights
+        double s = sw[V[i0]];
         int64_t j = i0 + 1;
         for (; j + 8 <= i1; j += 8) {
             double x[8];
 #pragma unroll
-            for (int t = 0; t < 8; t++) x[t] = gw[V[j + t]];
+            for (int t = 0; t < 8; t++) x[t] = sw[V[j + t]];
 #pragma unroll
             for (int t = 0; t < 8; t++) s = __dadd_rn(s, x[t]);
         }
-        for (; j < i1; j++) s = __dadd_rn(s, gw[V[j]]);
-        const int64_t o = rstart[big_row[q]] + (h - rowfirst[q]);
+        for (; j < i1; j++) s = __dadd_rn(s, sw[V[j]]);
+        const int64_t o = seg + (h - rowfirst[q]);
         uk[o] = (int32_t)(k & mask);
         uw[o] = s;
     }
@@ -484,13 +488,14 @@ __global__ void k_big_fold_long(const uint64_t *__restrict__ K, const uint32_t *
     for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < nl; r += nw) {
         const int64_t h = long_runs[r];
         const int64_t i0 = headpos[h], i1 = h + 1 < nheads ? headpos[h + 1] : m;
+        const double *__restrict__ sw = gw + rstart[big_row[K[i0] >> kbits]]; // segment's weights
         double ps[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         int64_t j = i0 + lane;
         for (; j + 7 * 32 < i1; j += 8 * 32) {
 #pragma unroll
-            for (int t = 0; t < 8; t++) ps[t] = __dadd_rn(ps[t], gw[V[j + t * 32]]);
+            for (int t = 0; t < 8; t++) ps[t] = __dadd_rn(ps[t], sw[V[j + t * 32]]);
         }
-        for (; j < i1; j += 32) ps[0] = __dadd_rn(ps[0], gw[V[j]]);
+        for (; j < i1; j += 32) ps[0] = __dadd_rn(ps[0], sw[V[j]]);
 #pragma unroll
         for (int t = 1; t < 8; t++) ps[0] = __dadd_rn(ps[0], ps[t]);
         double sum = ps[0];
@@ -675,6 +680,9 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
                                 ctx->stream));
         vg_sync(ctx);
         const int64_t nbig = ht[0], m = ht[1], nch = ht[2];
+        // the sort's payload indexes inside a segment, and no segment outgrows m
+        VG_REQUIRE(m <= (int64_t)UINT32_MAX, "aggregation sorts at most 2^32 - 1 entries (got %lld)",
+                   (long long)m);
         if (nbig > 0) {
             DevBuf<int32_t> big_row(ctx, nbig);
             { LaunchTimer lt(ctx);
