@@ -360,6 +360,13 @@ def test_bad_input_is_rejected(ctx):
         ctx.upload(np.array([0, 1], np.int64), np.array([5], np.int64), np.ones(1))
     with pytest.raises(vite_b200.VgError):
         ctx.upload(np.array([0, 2], np.int64), np.array([0], np.int64), np.ones(1))
+    # row offsets that decrease inside the array (first and last are right)
+    with pytest.raises(vite_b200.VgError):
+        ctx.upload(np.array([0, 2, 1, 3], np.int64), np.array([0, 1, 2], np.int64), np.ones(3))
+    # a row of more than 2^31 - 1 entries (the next offset then decreases as well)
+    with pytest.raises(vite_b200.VgError):
+        ctx.upload(np.array([0, 2 ** 31 + 5, 3], np.int64), np.array([0, 1, 1], np.int64),
+                   np.ones(3))
     g = upload(ctx, vo.rgg(100))
     with pytest.raises(vite_b200.VgError):
         ctx.louvain_phase(g, ordering=1)  # no coloring attached

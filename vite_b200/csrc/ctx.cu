@@ -237,6 +237,32 @@ void vg_graph_release(vg_ctx *ctx, vg_graph *g) {
     g->comm = nullptr;
 }
 
+namespace {
+// flags row offsets (n1 of them, the first taken as base) that decrease, hold a row of
+// more than INT32_MAX entries (degrees are 32-bit in the sweep), or do not end at base + ne
+__global__ void k_check_rowptr(const int64_t *__restrict__ rp, int64_t n1, int64_t base,
+                               int64_t ne, int *__restrict__ bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n1;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (i + 1 < n1) {
+            const int64_t len = rp[i + 1] - rp[i];
+            if (len < 0 || len > (int64_t)INT32_MAX) *bad = 1;
+        }
+        if (i == n1 - 1 && rp[i] - base != ne) *bad = 1;
+    }
+}
+} // namespace
+
+void vg_check_rowptr_async(vg_ctx *ctx, const int64_t *rp, int64_t n1, int64_t base, int64_t ne,
+                           int *bad) {
+    if (n1 <= 0) return;
+    {
+        LaunchTimer lt(ctx);
+        k_check_rowptr<<<vg_grid(ctx, n1, 256), 256, 0, ctx->stream>>>(rp, n1, base, ne, bad);
+    }
+    VG_CHECK_LAUNCH();
+}
+
 // Vite's 16-byte Edge records -> int32 tails + FP64 weights; flags tails out of range
 __global__ void k_split_edges(const vg_edge *__restrict__ e, int64_t ne, int64_t nv,
                               int32_t *__restrict__ tail, double *__restrict__ w,
@@ -278,12 +304,14 @@ extern "C" vg_status vg_graph_upload(vg_ctx *ctx, int64_t nv, int64_t ne, const 
         DevBuf<double> w(ctx, ne);
         VG_CUDA(cudaMemcpyAsync(rp.p, rowptr, sizeof(int64_t) * (nv + 1), cudaMemcpyHostToDevice,
                                 ctx->stream));
+        // bad[0]: row offsets, bad[1]: tails; read back together
+        DevBuf<int> bad(ctx, 2);
+        VG_CUDA(cudaMemsetAsync(bad.p, 0, 2 * sizeof(int), ctx->stream));
+        vg_check_rowptr_async(ctx, rp.p, nv + 1, 0, ne, bad.p);
         if (ne) {
             // stage the 16-byte records through a bounded device buffer in chunks
             const int64_t chunk = ne < (int64_t)(1 << 24) ? ne : (int64_t)(1 << 24);
             DevBuf<vg_edge> stage(ctx, chunk);
-            DevBuf<int> bad(ctx, 1);
-            VG_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
             for (int64_t off = 0; off < ne; off += chunk) {
                 const int64_t len = (ne - off) < chunk ? (ne - off) : chunk;
                 VG_CUDA(cudaMemcpyAsync(stage.p, edges + off, sizeof(vg_edge) * len,
@@ -291,15 +319,17 @@ extern "C" vg_status vg_graph_upload(vg_ctx *ctx, int64_t nv, int64_t ne, const 
                 {
                     LaunchTimer lt(ctx);
                     k_split_edges<<<vg_grid(ctx, len, 256), 256, 0, ctx->stream>>>(
-                        stage.p, len, nv, tail.p + off, w.p + off, bad.p);
+                        stage.p, len, nv, tail.p + off, w.p + off, bad.p + 1);
                 }
                 VG_CHECK_LAUNCH();
             }
-            int *hb = (int *)vg_pinned(ctx, sizeof(int));
-            VG_CUDA(cudaMemcpyAsync(hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-            vg_sync(ctx);
-            VG_REQUIRE(*hb == 0, "edge tail out of range [0, nv)");
         }
+        int *hb = (int *)vg_pinned(ctx, 2 * sizeof(int));
+        VG_CUDA(cudaMemcpyAsync(hb, bad.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        vg_sync(ctx);
+        VG_REQUIRE(hb[0] == 0, "rowptr must not decrease, and no row may hold more than 2^31 - 1 "
+                               "entries");
+        VG_REQUIRE(hb[1] == 0, "edge tail out of range [0, nv)");
         *out = vg_graph_wrap(ctx, nv, ne, rp.detach(), tail.detach(), w.detach());
     });
 }

@@ -21,17 +21,7 @@ namespace {
 
 constexpr size_t IO_CHUNK = 64ull << 20; // most bytes per pinned buffer (a multiple of 16)
 
-// flags row offsets (n1 of them, first = base) that decrease or do not end at base + ne
-__global__ void k_check_offsets(const int64_t *__restrict__ rp, int64_t n1, int64_t base,
-                                int64_t ne, int *__restrict__ bad) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n1;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        if (i + 1 < n1 && rp[i + 1] < rp[i]) *bad = 1;
-        if (i == n1 - 1 && rp[i] - base != ne) *bad = 1;
-    }
-}
-
-// rowptr -= base (after k_check_offsets has read them all)
+// rowptr -= base (after vg_check_rowptr_async has read them all)
 __global__ void k_rebase(int64_t *__restrict__ rp, int64_t n1, int64_t base) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n1;
          i += (int64_t)gridDim.x * blockDim.x)
@@ -153,12 +143,7 @@ extern "C" vg_status vg_graph_read_vite(vg_ctx *ctx, const char *path, vg_graph 
                                         cudaMemcpyHostToDevice, ctx->stream));
                 VG_CUDA(cudaEventRecord(done[b], ctx->stream));
             }
-            {
-                LaunchTimer lt(ctx);
-                k_check_offsets<<<vg_grid(ctx, nv + 1, 256), 256, 0, ctx->stream>>>(rp.p, nv + 1,
-                                                                                     base, ne, bad.p);
-            }
-            VG_CHECK_LAUNCH();
+            vg_check_rowptr_async(ctx, rp.p, nv + 1, base, ne, bad.p);
             if (base != 0) {
                 LaunchTimer lt(ctx);
                 k_rebase<<<vg_grid(ctx, nv + 1, 256), 256, 0, ctx->stream>>>(rp.p, nv + 1, base);
@@ -190,7 +175,8 @@ extern "C" vg_status vg_graph_read_vite(vg_ctx *ctx, const char *path, vg_graph 
             VG_CUDA(cudaMemcpyAsync(hbad, bad.p, 2 * sizeof(int), cudaMemcpyDeviceToHost,
                                     ctx->stream));
             vg_sync(ctx);
-            VG_REQUIRE(hbad[0] == 0, "%s: row offsets decrease or do not end at ne=%lld", path,
+            VG_REQUIRE(hbad[0] == 0, "%s: row offsets decrease, hold a row of 2^31 or more entries or "
+                                   "do not end at ne=%lld", path,
                        (long long)ne);
             VG_REQUIRE(hbad[1] == 0, "%s: an edge tail is outside [0, nv=%lld)", path,
                        (long long)nv);

@@ -159,6 +159,12 @@ inline bool vg_auto_layout(vg_ctx *ctx, const vg_graph *g, int mode) {
     return g->nv >= (1 << 18) && vg_local_structure(ctx, g);
 }
 
+// stream-ordered check of n1 row offsets (the first one is `base`): sets *bad (device
+// memory) when they decrease, a row holds more than INT32_MAX entries, or the last is
+// not base + ne
+void vg_check_rowptr_async(vg_ctx *ctx, const int64_t *rp, int64_t n1, int64_t base, int64_t ne,
+                           int *bad);
+
 void vg_graph_release(vg_ctx *ctx, vg_graph *g);
 // the graph takes ownership of the three arrays
 vg_graph *vg_graph_wrap(vg_ctx *ctx, int64_t nv, int64_t ne, int64_t *rowptr, int32_t *tail,
