@@ -150,7 +150,8 @@ vg_status vg_vertex_degree(vg_ctx *ctx, vg_graph *g, double *vdeg_out, double *c
  * while they run -- a server that reserved its whole memory budget at start-up, a
  * framework whose allocator owns the device memory, code that must not stall or fail
  * on an allocation mid-run. The caller passes device pointers: rowptr int64[nv+1]
- * and weights f64[ne] of a CSR, and vdeg_out f64[nv] for the degrees; 1/(2m) is
+ * and weights f64[ne] of a CSR (weights may be NULL only when the CSR holds no
+ * entries, else VG_ERR_ARG), and vdeg_out f64[nv] for the degrees; 1/(2m) is
  * written to *constant_out (host). Runs on `stream` (a cudaStream_t, NULL = default
  * stream) of the current device and returns after the stream has finished. The
  * scratch of the reduction is a file-scope device array of 512 KiB held by every GPU

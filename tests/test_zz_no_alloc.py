@@ -42,3 +42,30 @@ def test_noalloc_matches_vg_vertex_degree(maker):
             assert c == c_ref
         else:
             assert abs(c - c_ref) <= 1e-12 * abs(c_ref)
+
+
+@pytest.mark.gpu
+def test_null_weights_only_without_entries():
+    import torch
+
+    # a CSR without entries: NULL weights are accepted, every degree is zero and
+    # 1/(2m) is what vg_vertex_degree gives for the same graph
+    nv = 5
+    rowptr = np.zeros(nv + 1, np.int64)
+    with vite_b200.Context(0) as ctx:
+        vd_ref, c_ref = ctx.vertex_degree(ctx.upload(rowptr, np.zeros(0, np.int64), np.zeros(0)))
+    rp = torch.tensor(rowptr, device="cuda")
+    out = torch.full((nv,), float("nan"), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    c = vite_b200.vertex_degree_noalloc(nv, rp.data_ptr(), 0, out.data_ptr(), stream)
+    np.testing.assert_array_equal(out.cpu().numpy(), vd_ref)
+    assert c == c_ref
+    # a CSR with entries and NULL weights: rejected before any kernel runs
+    g = vo.rgg(4096)
+    rp = torch.tensor(g.rowptr, dtype=torch.int64, device="cuda")
+    out = torch.full((g.nv,), float("nan"), dtype=torch.float64, device="cuda")
+    with pytest.raises(vite_b200.VgError) as ei:
+        vite_b200.vertex_degree_noalloc(g.nv, rp.data_ptr(), 0, out.data_ptr(), stream)
+    assert ei.value.status == vite_b200.VG_ERR_ARG
+    assert "NULL" in str(ei.value)
+    assert torch.isnan(out).all().item()

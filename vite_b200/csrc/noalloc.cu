@@ -63,7 +63,8 @@ __global__ void __launch_bounds__(NA_THREADS) k_na_degree(const int64_t *__restr
         if (v >= nv) break;
         double tw = 0.0;
         const int64_t e1 = rowptr[v + 1];
-        for (int64_t e = rowptr[v]; e < e1; e++) tw = __dadd_rn(tw, w[e]);
+        if (w) // null only for a CSR without entries (checked on the host)
+            for (int64_t e = rowptr[v]; e < e1; e++) tw = __dadd_rn(tw, w[e]);
         vdeg[v] = tw;
         s = __dadd_rn(s, tw);
     }
@@ -128,6 +129,27 @@ extern "C" vg_status vg_vertex_degree_noalloc(int64_t nv, const int64_t *d_rowpt
         scratch = g_noalloc_addr[dev];
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!d_weight) {
+        // no weights: allowed for a CSR without entries only (rowptr[0] == rowptr[nv]);
+        // two 8-byte reads into host stack memory, nothing allocated
+        int64_t ends[2] = {0, 0};
+        e = cudaMemcpyAsync(&ends[0], d_rowptr, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&ends[1], d_rowptr + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            snprintf(msg, sizeof(msg), "vg_vertex_degree_noalloc: %s", cudaGetErrorString(e));
+            set_err(errbuf, errlen, msg);
+            return VG_ERR_CUDA;
+        }
+        if (ends[1] != ends[0]) {
+            snprintf(msg, sizeof(msg),
+                     "vg_vertex_degree_noalloc: d_weight is NULL but the CSR holds %lld entries",
+                     (long long)(ends[1] - ends[0]));
+            set_err(errbuf, errlen, msg);
+            return VG_ERR_ARG;
+        }
+    }
     const int ntiles = (int)((nv + NA_TILE - 1) / NA_TILE);
     k_na_degree<<<ntiles, NA_THREADS, 0, s>>>(d_rowptr, d_weight, nv, d_vdeg_out, scratch);
     k_na_constant<<<1, NA_THREADS, 0, s>>>(scratch, ntiles, scratch + NA_MAX_TILES);
