@@ -5,14 +5,20 @@ sweeps, community updates, modularity, rebuild) over the graph, through
 vg_louvain_run. `value` is seconds per step with the graph already resident in
 HBM (device-timed with CUDA events on the library's stream); `e2e` is the same
 step through the C ABI from pinned host buffers in Vite's layout, the H2D copy of
-the CSR and the D2H read of the per-level results inside the timed region.
+the CSR, the per-iteration read-backs and the D2H copy of the -o map (every input
+vertex's final community, what distLouvainMethod's caller gets back) inside the
+timed region. The reference (oracle/_ref, the unmodified Vite sources) runs once on
+the same graph for the CPU baseline, and every level is compared with ours; the
+skewed-degree configuration (Barabasi-Albert 4M, -c 8 -t 2 -a 0.25) follows as a
+sub-record with its own reference run, then the batched and served forms.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 With N > 1 (torchrun, one rank per GPU) every rank runs its own replica of the
 workload (the path does not shard: one graph lives on one GPU); rank 0 prints
 the max over ranks. --impl reference times the reference's own CPU code
-(oracle/_ref, built from the reference sources) on the host cores.
+(oracle/_ref) on the host cores on the full graph, generated on the host by the
+oracle's generator, without loading the library under test.
 """
 from __future__ import annotations
 
@@ -34,7 +40,7 @@ N_VERTICES = 1 << 24
 EXTRA_PERCENT = 1.0
 SEED = 2024
 THRESHOLD = 1e-6
-SAMPLE_VERTICES = 1 << 20  # CPU-baseline sample (same generator, same seed)
+REF_BUDGET_S = 1400.0      # reference arm: its timed runs end within this many seconds of its start
 METRIC = "Louvain e2e sec (RGG 2^24 +1% extra edges, full multi-level)"
 UNIT = "s"
 
@@ -68,8 +74,7 @@ def parse():
     ap.add_argument("--skip-batched", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--skip-serving", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--serve-lanes", type=str, default=None, help=argparse.SUPPRESS)
-    ap.add_argument("--check-reference", action="store_true",
-                    help="also run the reference on the full graph and compare every level")
+    ap.add_argument("--skip-ba", action="store_true", help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -171,60 +176,132 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------
-# CPU baseline: the reference's own code (oracle/_ref) on a bounded sample
+# the reference's own code (oracle/_ref, the unmodified Vite sources) on the host cores
 
 
-def reference_sample_seconds(ctx, threads: int, n_sample: int) -> tuple[float, int, str]:
-    """Run the reference binary on an RGG sample written in Vite's binary format;
-    returns (seconds of clustering + rebuild, CSR entries of the sample, kind)."""
+def cpu_info() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_rgg_file(path: str, n: int) -> tuple[int, int]:
+    """The benchmark graph built on the host by the oracle's generator (bit-identical to
+    the device generator: same LCG points, same radius test, same seeded extra edges) and
+    written as a Vite binary file; returns (vertices, CSR entries)."""
     from oracle import vite_oracle as vo
 
-    g = ctx.generate_rgg(n_sample, EXTRA_PERCENT, SEED)
-    rp, tail, w = g.download()
-    g.free()
-    sample = vo.Graph(rp, tail, w)
-    if os.path.exists(vo.HARNESS):
-        with tempfile.TemporaryDirectory() as tmp:
-            path = os.path.join(tmp, "sample.bin")
-            vo.write_vite_binary(path, sample)
-            out = vo.run_harness(["-f", path], os.path.join(tmp, "s.rec"), threads=threads,
-                                 timeout=600)
-        tot = [l for l in out.splitlines() if l.startswith("HARNESS total_clustering_s")][0].split()
-        return float(tot[6]), sample.ne, "reference"
-    r = vo.run(sample)  # restatement (single thread) when the reference build is absent
-    return r.seconds, sample.ne, "port"
+    g = vo.rgg(n)
+    x, _ = vo.add_random_edges(g, EXTRA_PERCENT, SEED)
+    del g
+    vo.write_vite_binary(path, x)
+    return x.nv, x.ne
 
 
 def run_reference_arm(args, rank: int, ws: int) -> None:
-    """--impl reference: the reference's CPU implementation on the host cores."""
+    """--impl reference: the reference's CPU implementation (graphClustering's phase loop
+    over the unmodified Vite sources, oracle/_ref/vite_ref_harness, all host threads) on
+    the full benchmark graph. The graph is generated on the host and written once; the
+    harness reads it once and runs the whole level loop K times, each run on a fresh copy
+    of the level-0 graph; a step is one run (clustering + rebuild of every level, as
+    graphClustering reports them). Runs stop early, and the line says so, when one more
+    would end past REF_BUDGET_S. This process never loads the library under test."""
     if rank != 0:
         return
-    import vite_b200
+    from oracle import vite_oracle as vo
+
     threads = os.cpu_count() or 1
-    ctx = vite_b200.Context(int(os.environ.get("LOCAL_RANK", "0")))
-    full = ctx.generate_rgg(args.n, EXTRA_PERCENT, SEED)
-    e_full = full.ne
-    full.free()
-    for _ in range(args.warmup):
-        reference_sample_seconds(ctx, threads, 1 << 14)
-    secs = []
-    kind, e_s = "reference", 1
-    for _ in range(args.steps):
-        s, e_s, kind = reference_sample_seconds(ctx, threads, SAMPLE_VERTICES)
-        secs.append(s)
-    ctx.close()
-    per = statistics.mean(secs) * e_full / e_s
-    sample = (f"RGG n={SAMPLE_VERTICES} +{EXTRA_PERCENT:g}% (E={e_s}) full multi-level Louvain "
-              f"(clustering + rebuild, graph load excluded), mean of {len(secs)} runs "
-              f"({statistics.mean(secs):.3f} s), scaled by CSR entries to E={e_full}")
-    line = {"metric": METRIC, "value": per, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+    t_arm = time.perf_counter()
+    if not os.path.exists(vo.HARNESS):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/vite_ref_harness was not built (reference sources absent)"}),
+              flush=True)
+        return
+    with tempfile.TemporaryDirectory() as tmp:
+        warm = os.path.join(tmp, "warm.bin")
+        cpu_rgg_file(warm, 1 << 16)
+        vo.run_harness(["-f", warm, "-r", str(args.warmup)], None, threads=threads, timeout=600)
+        path = os.path.join(tmp, "rgg.bin")
+        t0 = time.perf_counter()
+        nv, ne = cpu_rgg_file(path, args.n)
+        gen_s = time.perf_counter() - t0
+        budget = max(REF_BUDGET_S - (time.perf_counter() - t_arm), 60.0)
+        out = vo.run_harness(["-f", path, "-r", str(args.steps), "-B", f"{budget:.0f}"], None,
+                             threads=threads, timeout=budget + 900)
+    runs = vo.harness_totals(out)
+    secs = [r["total_s"] for r in runs]
+    per = statistics.mean(secs)
+    sample = (f"the full workload: RGG n={nv} +{EXTRA_PERCENT:g}% extra edges, E={ne} CSR "
+              f"entries, generated on the host by the oracle's generator (bit-identical to the "
+              f"device generator) and read once from a Vite binary file; each step one whole "
+              f"graphClustering level loop (clustering + rebuild, {runs[0]['levels']} levels, "
+              f"{runs[0]['iterations']} iterations) on a fresh copy of the graph; mean of "
+              f"{len(secs)} runs; {threads} OpenMP threads on {cpu_info()}")
+    line = {"metric": METRIC, "value": per, "unit": UNIT, "n_gpus": ws, "steps": len(secs),
             "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(args.n), "impl": "reference",
-            "cpu_baseline": {"value": per, "unit": UNIT, "cores": threads, "kind": kind,
+            "cpu_baseline": {"value": per, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": sample},
-            "e2e": {"value": per, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": per, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "run_seconds": secs, "final_modularity": runs[-1]["final_mod"],
+            "graph_read_s": vo.harness_read_seconds(out), "generate_s": gen_s,
+            "warmup_runs": f"{args.warmup} level loops on RGG n=65536 (same generator)"}
+    if len(secs) < args.steps:
+        line["steps_requested"] = args.steps
+        line["note"] = (f"{len(secs)} of {args.steps} runs: one more would have ended past the "
+                        f"{REF_BUDGET_S:.0f} s budget of this arm")
     print(json.dumps(line), flush=True)
+
+
+def reference_levels(path: str, flags: list, threads: int) -> tuple[list, dict]:
+    """One reference run (oracle/_ref, all host threads) on a Vite binary file: its
+    recorded levels and its totals."""
+    from oracle import vite_oracle as vo
+
+    with tempfile.TemporaryDirectory() as tmp:
+        rec = os.path.join(tmp, "ref.rec")
+        out = vo.run_harness(["-f", path, *flags], rec, threads=threads, timeout=3600)
+        levels = vo.read_record(rec).levels
+    tot = vo.harness_totals(out)[0]
+    tot["read_s"] = vo.harness_read_seconds(out)
+    return levels, tot
+
+
+def level_parity(ours: list, ref_levels: list, our_map, ctx, exact: bool) -> dict:
+    """Per level: vertices, entries, iterations and modularity, ours against the reference's;
+    and the -o maps (graphClustering's final communities of every input vertex)."""
+    from oracle import vite_oracle as vo
+
+    ref = [lv for lv in ref_levels if lv.level >= 0]
+    per = []
+    for a, b in zip(ours, ref):
+        per.append({"nv": [a["nv"], b.nv], "ne": [a["ne"], b.ne], "iters": [a["iters"], b.iters],
+                    "modularity": [a["modularity"], b.mod],
+                    "rel_diff": abs(a["modularity"] - b.mod) / abs(b.mod) if b.mod else 0.0,
+                    "bits_equal": float(a["modularity"]).hex() == float(b.mod).hex()})
+    same_shape = len(ours) == len(ref) and all(
+        p["nv"][0] == p["nv"][1] and p["ne"][0] == p["ne"][1] and p["iters"][0] == p["iters"][1]
+        for p in per)
+    out = {"levels": [len(ours), len(ref)], "same_levels_entries_iterations": same_shape,
+           "max_rel_modularity_diff": max(p["rel_diff"] for p in per) if per else None,
+           "every_modularity_bit_identical": all(p["bits_equal"] for p in per),
+           "per_level": per}
+    ref_map = vo.output_map(ref_levels)
+    if our_map is not None and ref_map is not None:
+        cmp = ctx.compare_communities(ref_map, our_map)
+        out["output_map"] = {"identical": bool(np.array_equal(ref_map, our_map)),
+                             **{k: cmp[k] for k in ("nc1", "nc2", "precision", "recall",
+                                                    "fscore")}}
+    out["bar"] = ("bit-identical levels (unit weights)" if exact else
+                  f"per-level modularity within {REL_TOL:g} relative (real weights)")
+    out["pass"] = bool(same_shape and (out["every_modularity_bit_identical"] if exact else
+                                      (out["max_rel_modularity_diff"] or 0.0) <= REL_TOL))
+    return out
 
 
 # ---------------------------------------------------------------------------------------
@@ -409,43 +486,90 @@ def run_serving(ctx, count: int, lanes=SERVE_LANES) -> dict:
     }
 
 
-def check_reference_full(ctx, g, rp, ed, ours: list) -> dict:
-    """The reference (oracle/_ref, all host threads) on the full benchmark graph,
-    read from a Vite binary file: per-level vertices, entries, iterations and
-    modularity against ours, and the level-0 partitions compared with the device
-    ground-truth comparison (the reference as truth)."""
+def write_vite_file(path: str, rp: np.ndarray, ed: np.ndarray) -> None:
+    """Vite's binary layout: nv, ne, rowptr[nv+1], Edge{int64 tail, double weight}[ne]."""
     import struct
 
-    from oracle import vite_oracle as vo
+    with open(path, "wb") as f:
+        f.write(struct.pack("<qq", len(rp) - 1, len(ed)))
+        np.ascontiguousarray(rp, dtype="<i8").tofile(f)
+        ed.tofile(f)
 
-    threads = os.cpu_count() or 1
-    with tempfile.TemporaryDirectory() as tmp:
-        path = os.path.join(tmp, "rgg.bin")
-        with open(path, "wb") as f:  # Vite's binary layout: nv, ne, rowptr, Edge records
-            f.write(struct.pack("<qq", len(rp) - 1, len(ed)))
-            np.ascontiguousarray(rp, dtype="<i8").tofile(f)
-            ed.tofile(f)
-        rec = os.path.join(tmp, "ref.rec")
-        t0 = time.perf_counter()
-        vo.run_harness(["-f", path], rec, threads=threads, timeout=3600)
-        ref_s = time.perf_counter() - t0
-        r = vo.read_record(rec)
-    ref_levels = [lv for lv in r.levels if lv.level >= 0]
-    per = []
-    for a, b in zip(ours, ref_levels):
-        per.append({"nv": [a["nv"], b.nv], "ne": [a["ne"], b.ne], "iters": [a["iters"], b.iters],
-                    "modularity": [a["modularity"], b.mod],
-                    "rel_diff": abs(a["modularity"] - b.mod) / abs(b.mod)})
-    cv0, _, _ = ctx.louvain_phase(g, threshold=THRESHOLD)
-    cmp0 = ctx.compare_communities(ref_levels[0].cvect, cv0)
-    return {"reference": f"oracle/_ref/vite_ref_harness -f <graph> ({threads} threads), "
-                         f"{ref_s:.1f} s wall including the file read",
-            "levels": [len(ours), len(ref_levels)],
-            "max_rel_modularity_diff": max(p["rel_diff"] for p in per),
-            "final_modularity": [ours[-1]["modularity"], ref_levels[-1].mod],
-            "level0_partition_vs_reference": {k: cmp0[k] for k in ("nc1", "nc2", "precision",
-                                                                   "recall", "fscore")},
-            "per_level": per}
+
+# the skewed-degree configuration: Barabasi-Albert, unit weights, coloring + ET
+BA_N, BA_M, BA_SEED = 4_194_304, 8, 1
+BA_FLAGS = ["-c", "8", "-t", "2", "-a", "0.25"]
+BA_KW = {"coloring": True, "max_colors": 8, "et_type": 2, "et_delta": 0.25}
+BA_STEPS = 10
+
+
+def run_ba_config(ctx, stream, args) -> dict:
+    """Barabasi-Albert n=4,194,304, m=8 (seed 1), unit FP64 weights, graphClustering
+    -c 8 -t 2 -a 0.25 (distance-1 coloring, early termination alpha 0.25): device-resident
+    and end-to-end times, and the reference's own run on the same graph (oracle/_ref, all
+    host threads) with every level compared bit for bit (unit weights: every sum is exact)."""
+    import torch
+
+    import vite_b200
+
+    g = ctx.generate_ba(BA_N, BA_M, BA_SEED)
+    nv, ne = g.nv, g.ne
+    rp_h, tail_h, w_h = g.download()
+    rp_pin = torch.empty(nv + 1, dtype=torch.int64, pin_memory=True)
+    ed_pin = torch.empty(ne * 2, dtype=torch.int64, pin_memory=True)
+    rp_pin.numpy()[:] = rp_h
+    ed = ed_pin.numpy().view(vite_b200.EDGE_DTYPE)
+    ed["tail"] = tail_h
+    ed["weight"] = w_h
+    del rp_h, tail_h, w_h
+    comm_pin = torch.empty(nv, dtype=torch.int64, pin_memory=True)
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1) * 1e-3 / k
+
+    def e2e():
+        h = ctx.upload_edges(rp_pin.numpy(), ed)
+        r = ctx.run(h, threshold=THRESHOLD, comm_out=comm_pin.numpy(), **BA_KW)
+        h.free()
+        return r
+
+    for _ in range(3):
+        ctx.run(g, threshold=THRESHOLD, **BA_KW)
+    dev, t_dev = timed(lambda: ctx.run(g, threshold=THRESHOLD, **BA_KW), BA_STEPS)
+    e2e()
+    res, t_e2e = timed(e2e, BA_STEPS)
+    out = {"workload": f"Barabasi-Albert n={nv} m={BA_M} (seed {BA_SEED}), unit FP64 weights, "
+                       f"graphClustering {' '.join(BA_FLAGS)} (coloring with 4 hash rounds, "
+                       f"early termination alpha 0.25), threshold {THRESHOLD:g}",
+           "nv": nv, "ne": ne, "seconds": t_dev, "e2e_seconds": t_e2e, "steps": BA_STEPS,
+           "e2e_bytes": {"h2d": 8 * (nv + 1) + 16 * ne,
+                         "d2h": 8 * nv + 16 * sum(s["iters"] for s in res.stats)},
+           "levels": [{"nv": s["nv"], "ne": s["ne"], "iters": s["iters"],
+                       "modularity": s["modularity"], "colors": s["num_colors"],
+                       "color_s": s["seconds_color"], "phase_s": s["seconds_phase"],
+                       "rebuild_s": s["seconds_rebuild"]} for s in dev.stats]}
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, "ba.bin")
+            write_vite_file(path, rp_pin.numpy(), ed)
+            ref_lv, tot = reference_levels(path, BA_FLAGS, threads)
+        out["reference_seconds"] = tot["total_s"]
+        out["reference"] = (f"oracle/_ref/vite_ref_harness -f <graph> {' '.join(BA_FLAGS)}, "
+                            f"{threads} OpenMP threads on {cpu_info()}: clustering "
+                            f"{tot['clustering_s']:.2f} s + rebuild {tot['rebuild_s']:.2f} s "
+                            f"(graph read {tot['read_s']:.1f} s excluded)")
+        out["parity"] = level_parity(res.stats, ref_lv, comm_pin.numpy(), ctx, exact=True)
+        out["e2e_speedup_vs_reference"] = tot["total_s"] / t_e2e
+    g.free()
+    return out
 
 
 def main() -> None:
@@ -483,13 +607,15 @@ def main() -> None:
     ed["tail"] = tail_h
     ed["weight"] = w_h
     del rp_h, tail_h, w_h
+    # the -o map (final community of every input vertex) comes back here in the e2e leg
+    comm_pin = torch.empty(nv, dtype=torch.int64, pin_memory=True)
 
     def step_device():
         return ctx.run(g, threshold=THRESHOLD)
 
     def step_e2e():
         h = ctx.upload_edges(rp_pin.numpy(), ed)
-        res = ctx.run(h, threshold=THRESHOLD)
+        res = ctx.run(h, threshold=THRESHOLD, comm_out=comm_pin.numpy())
         h.free()
         return res
 
@@ -530,7 +656,7 @@ def main() -> None:
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        step_e2e()
+        res_e2e = step_e2e()
     e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize()
@@ -559,14 +685,25 @@ def main() -> None:
         tj = json.load(open(tpath))
         traffic = tj.get("dram_bytes_per_sweep_level0")
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        # the reference (oracle/_ref, all host threads) once on the whole benchmark graph,
+        # read from a Vite binary file: its time is the CPU baseline, its levels and -o map
+        # are compared with ours
         threads = os.cpu_count() or 1
-        s, e_s, kind = reference_sample_seconds(ctx, threads, SAMPLE_VERTICES)
-        cpu = {"value": s * ne / e_s, "unit": UNIT, "cores": threads if kind == "reference" else 1,
-               "kind": kind,
-               "sample": f"RGG n={SAMPLE_VERTICES} +{EXTRA_PERCENT:g}% (E={e_s}), full multi-level "
-                         f"Louvain measured {s:.3f} s, scaled by CSR entries to E={ne}"}
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, "rgg.bin")
+            write_vite_file(path, rp_pin.numpy(), ed)
+            ref_lv, tot = reference_levels(path, [], threads)
+        cpu = {"value": tot["total_s"], "unit": UNIT, "cores": threads, "kind": "reference",
+               "sample": f"the full workload once (E={ne}): graphClustering's level loop over "
+                         f"the unmodified Vite sources (oracle/_ref), clustering "
+                         f"{tot['clustering_s']:.2f} s + rebuild {tot['rebuild_s']:.2f} s, "
+                         f"{tot['levels']} levels; graph read from a Vite binary file "
+                         f"({tot['read_s']:.1f} s, excluded); {threads} OpenMP threads on "
+                         f"{cpu_info()}"}
+        parity = level_parity(res_e2e.stats, ref_lv, comm_pin.numpy(), ctx, exact=False)
+        del ref_lv
 
     line = {
         "metric": METRIC, "value": per_step, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -587,15 +724,20 @@ def main() -> None:
                      "kernel": "local-moving sweep (all degree-class launches of one iteration), "
                                f"level 0; algorithmic bytes 16*E+48*V = {sweep_bytes}; "
                                f"peak {peak_src}"},
-        # D2H per step: the modularity + frozen-count read-back (16 B) of every iteration
+        # D2H per step: the -o map (8 B per input vertex) and the modularity +
+        # frozen-count read-back (16 B) of every iteration
         "e2e": {"value": per_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * (nv + 1) + 16 * ne,
-                "d2h_bytes_per_step": 16 * sum(s["iters"] for s in last)},
+                "d2h_bytes_per_step": 8 * nv + 16 * sum(s["iters"] for s in res_e2e.stats)},
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
-    if ws == 1 and args.check_reference:
-        line["check_reference"] = check_reference_full(ctx, g, rp_pin.numpy(), ed, last)
+    if parity is not None:
+        line["reference_parity"] = parity
+    g.free()
+    del rp_pin, ed_pin, ed, comm_pin
+    if ws == 1 and not args.skip_ba:
+        line["ba_config"] = run_ba_config(ctx, stream, args)
     if ws == 1 and not args.skip_batched:
         line["batched"] = run_batched(ctx, stream, args.batch_graphs)
     if ws == 1 and not args.skip_serving:
@@ -604,7 +746,6 @@ def main() -> None:
         line["serving"] = run_serving(ctx, args.serve_requests, lanes)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    g.free()
     ctx.close()
     if ws > 1:
         dist.destroy_process_group()

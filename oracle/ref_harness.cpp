@@ -10,6 +10,11 @@
 // level's result (community vector, modularity printed with all 17 digits,
 // iteration count, colors) and, on request, the CSR each level ran on, in a small
 // binary record file that the parity tests and the golden-fixture script read.
+// With -r R it runs the whole level loop R times, each run on a copy of the
+// loaded graph made before its clock starts, and prints each run's totals
+// (clustering + rebuild seconds, as main's "Average time for clustering" and
+// "Rebuild Time" lines add up); -B stops before a run that would end past a
+// budget of seconds. Only the first run is recorded.
 //
 // Record file layout (little endian):
 //   header  : "VREC" u32 version=1
@@ -50,13 +55,16 @@ struct Opts {
   bool thresholdScaling = false, runOnePhase = false;
   double threshold = CONVERGENCE_THRESHOLD;
   bool dumpGraphs = false;
+  int repeats = 1;          // timed runs of the whole level loop from the loaded graph
+  double budget = 0.0;      // seconds; 0 = no limit on the repeats
 };
 
 static void usage()
 {
   std::fprintf(stderr,
       "vite_ref_harness (-n N [-e pct] [-s save.bin] | -f file) [-u] [-c \"k [single]\"]\n"
-      "  [-d \"k [single]\"] [-t type] [-a alpha] [-i] [-p] [-h thresh] [-w out.rec] [-G]\n");
+      "  [-d \"k [single]\"] [-t type] [-a alpha] [-i] [-p] [-h thresh] [-w out.rec] [-G]\n"
+      "  [-r repeats] [-B budget_seconds]\n");
   std::exit(2);
 }
 
@@ -89,57 +97,15 @@ static void recordGraph(long long level, const DistGraph &dg)
   std::fwrite(w.data(), sizeof(double), ne, g_rec);
 }
 
-int main(int argc, char **argv)
+struct RunTotals {
+  double clustering = 0.0, rebuild = 0.0, finalMod = 0.0;
+  int levels = 0, iterations = 0;
+};
+
+// One run of main's phase loop (main.cpp:242-513) on dg, which the rebuilds
+// replace (rebuild.cpp:334) and which is deleted at the end.
+static RunTotals runLevels(int me, int nprocs, DistGraph *dg, const Opts &o)
 {
-  MPI_Init(&argc, &argv);
-  int me = 0, nprocs = 1;
-  MPI_Comm_rank(MPI_COMM_WORLD, &me);
-  MPI_Comm_size(MPI_COMM_WORLD, &nprocs);
-
-  Opts o;
-  for (int i = 1; i < argc; i++) {
-    std::string a(argv[i]);
-    auto need = [&](void) -> const char * { if (i + 1 >= argc) usage(); return argv[++i]; };
-    if (a == "-n") o.genN = std::atoll(need());
-    else if (a == "-e") o.randomEdgePercent = std::atof(need());
-    else if (a == "-s") o.saveGraph = need();
-    else if (a == "-f") o.inFile = need();
-    else if (a == "-u") o.unitWeights = true;
-    else if (a == "-c") { parseColor(need(), o); o.coloring = true; }
-    else if (a == "-d") { parseColor(need(), o); o.vertexOrdering = true; }
-    else if (a == "-t") { o.earlyTerm = true; o.etType = std::atoi(need()); }
-    else if (a == "-a") o.etDelta = std::atof(need());
-    else if (a == "-i") o.thresholdScaling = true;
-    else if (a == "-p") o.runOnePhase = true;
-    else if (a == "-h") o.threshold = std::atof(need());
-    else if (a == "-w") o.recFile = need();
-    else if (a == "-G") o.dumpGraphs = true;
-    else usage();
-  }
-  if (o.genN == 0 && o.inFile.empty()) usage();
-
-  createCommunityMPIType();
-  createEdgeMPIType();
-
-  DistGraph *dg = nullptr;
-  double tg0 = MPI_Wtime();
-  if (o.genN > 0)
-    generateInMemGraph(me, nprocs, dg, o.genN, o.randomEdgePercent, o.saveGraph);
-  else
-    loadDistGraphMPIIO(me, nprocs, 1, dg, o.inFile);
-  double tg1 = MPI_Wtime();
-  if (o.unitWeights) dg->getLocalGraph().setEdgeWeightstoOne();
-  std::printf("HARNESS graph_seconds %.6f nv %lld ne %lld threads %d\n", tg1 - tg0,
-              (long long)dg->getTotalNumVertices(),
-              (long long)dg->getLocalGraph().getNumEdges(), omp_get_max_threads());
-
-  if (!o.recFile.empty()) {
-    g_rec = std::fopen(o.recFile.c_str(), "wb");
-    if (!g_rec) { std::perror("record file"); return 1; }
-    std::fwrite("VREC", 1, 4, g_rec);
-    put<unsigned>(1);
-  }
-
   GraphWeight currMod = -1.0, prevMod = -1.0, threshold = o.threshold;
   int phase = 0, short_phase = 0, iters = 0, tot_iters = 0;
   ColorElem numColors = 0;
@@ -239,11 +205,93 @@ int main(int argc, char **argv)
     if (phase == TERMINATION_PHASE_COUNT || tot_iters > 10000) break;
   }
 
-  std::printf("HARNESS total_clustering_s %.6f total_rebuild_s %.6f total_s %.6f levels %d iterations %d final_mod %.17g\n",
-              totalClustering, totalRebuild, totalClustering + totalRebuild, phase, tot_iters,
-              (double)prevMod);
-  if (g_rec) { put<int>(0); std::fclose(g_rec); }
+  RunTotals t;
+  t.clustering = totalClustering;
+  t.rebuild = totalRebuild;
+  t.levels = phase;
+  t.iterations = tot_iters;
+  t.finalMod = prevMod;
   delete dg;
+  return t;
+}
+
+int main(int argc, char **argv)
+{
+  MPI_Init(&argc, &argv);
+  int me = 0, nprocs = 1;
+  MPI_Comm_rank(MPI_COMM_WORLD, &me);
+  MPI_Comm_size(MPI_COMM_WORLD, &nprocs);
+
+  Opts o;
+  for (int i = 1; i < argc; i++) {
+    std::string a(argv[i]);
+    auto need = [&](void) -> const char * { if (i + 1 >= argc) usage(); return argv[++i]; };
+    if (a == "-n") o.genN = std::atoll(need());
+    else if (a == "-e") o.randomEdgePercent = std::atof(need());
+    else if (a == "-s") o.saveGraph = need();
+    else if (a == "-f") o.inFile = need();
+    else if (a == "-u") o.unitWeights = true;
+    else if (a == "-c") { parseColor(need(), o); o.coloring = true; }
+    else if (a == "-d") { parseColor(need(), o); o.vertexOrdering = true; }
+    else if (a == "-t") { o.earlyTerm = true; o.etType = std::atoi(need()); }
+    else if (a == "-a") o.etDelta = std::atof(need());
+    else if (a == "-i") o.thresholdScaling = true;
+    else if (a == "-p") o.runOnePhase = true;
+    else if (a == "-h") o.threshold = std::atof(need());
+    else if (a == "-w") o.recFile = need();
+    else if (a == "-G") o.dumpGraphs = true;
+    else if (a == "-r") o.repeats = std::atoi(need());
+    else if (a == "-B") o.budget = std::atof(need());
+    else usage();
+  }
+  if (o.genN == 0 && o.inFile.empty()) usage();
+
+  createCommunityMPIType();
+  createEdgeMPIType();
+
+  DistGraph *dg = nullptr;
+  double tg0 = MPI_Wtime();
+  if (o.genN > 0)
+    generateInMemGraph(me, nprocs, dg, o.genN, o.randomEdgePercent, o.saveGraph);
+  else
+    loadDistGraphMPIIO(me, nprocs, 1, dg, o.inFile);
+  double tg1 = MPI_Wtime();
+  if (o.unitWeights) dg->getLocalGraph().setEdgeWeightstoOne();
+  std::printf("HARNESS graph_seconds %.6f nv %lld ne %lld threads %d\n", tg1 - tg0,
+              (long long)dg->getTotalNumVertices(),
+              (long long)dg->getLocalGraph().getNumEdges(), omp_get_max_threads());
+
+  if (!o.recFile.empty()) {
+    g_rec = std::fopen(o.recFile.c_str(), "wb");
+    if (!g_rec) { std::perror("record file"); return 1; }
+    std::fwrite("VREC", 1, 4, g_rec);
+    put<unsigned>(1);
+  }
+
+  // -r R: R timed runs of the level loop, each from a copy of the loaded graph
+  // made before its clock starts (the loaded graph itself runs last); -B stops
+  // before a run that would end past the budget, counted from the first run.
+  const int repeats = o.repeats > 0 ? o.repeats : 1;
+  double tStart = MPI_Wtime(), spent = 0.0;
+  for (int r = 0; r < repeats; r++) {
+    if (r > 0 && o.budget > 0.0) {
+      const double elapsed = MPI_Wtime() - tStart;
+      if (elapsed + spent / r > o.budget) {
+        std::printf("HARNESS budget_stop after %d runs elapsed_s %.3f\n", r, elapsed);
+        break;
+      }
+    }
+    DistGraph *run = (r + 1 < repeats) ? new DistGraph(*dg) : dg;
+    RunTotals t = runLevels(me, nprocs, run, o);
+    spent += t.clustering + t.rebuild;
+    std::printf("HARNESS total_clustering_s %.6f total_rebuild_s %.6f total_s %.6f levels %d iterations %d final_mod %.17g\n",
+                t.clustering, t.rebuild, t.clustering + t.rebuild, t.levels, t.iterations,
+                t.finalMod);
+    std::fflush(stdout);
+    if (g_rec) { put<int>(0); std::fclose(g_rec); g_rec = nullptr; }
+    if (run == dg) dg = nullptr;  // the last run consumed the loaded graph
+  }
+  if (dg) delete dg;
   destroyCommunityMPIType();
   destroyEdgeMPIType();
   MPI_Finalize();

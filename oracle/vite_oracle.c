@@ -122,27 +122,79 @@ double vo_rgg_radius(int64_t n)
 }
 
 typedef struct { int64_t src, dst; double w; } vo_trip;
+typedef struct { int64_t dst; double w; } vo_half;
 
-static int trip_cmp(const void *a, const void *b)
+static int half_cmp(const void *a, const void *b)
 {
-    const vo_trip *x = (const vo_trip *)a, *y = (const vo_trip *)b;
-    if (x->src != y->src) return x->src < y->src ? -1 : 1;
-    if (x->dst != y->dst) return x->dst < y->dst ? -1 : 1;
-    return 0;
+    const vo_half *x = (const vo_half *)a, *y = (const vo_half *)b;
+    return x->dst < y->dst ? -1 : (x->dst > y->dst ? 1 : 0);
 }
 
-/* CSR sorted by (src, dst) from a triple list (distgraph.cpp:899-952 order). */
-static int csr_from_triples(int64_t n, vo_trip *t, int64_t m, vo_graph *out)
+/* Sort one row's (tail, weight) pairs by tail: insertion sort for short rows,
+ * qsort through a scratch array for long ones. */
+static void sort_row(int64_t *tail, double *w, int64_t len, vo_half *scratch)
 {
-    qsort(t, (size_t)m, sizeof(vo_trip), trip_cmp);
+    if (len <= 48) {
+        for (int64_t a = 1; a < len; a++) {
+            const int64_t t = tail[a];
+            const double x = w[a];
+            int64_t b = a - 1;
+            while (b >= 0 && tail[b] > t) {
+                tail[b + 1] = tail[b];
+                w[b + 1] = w[b];
+                b--;
+            }
+            tail[b + 1] = t;
+            w[b + 1] = x;
+        }
+        return;
+    }
+    for (int64_t a = 0; a < len; a++) { scratch[a].dst = tail[a]; scratch[a].w = w[a]; }
+    qsort(scratch, (size_t)len, sizeof(vo_half), half_cmp);
+    for (int64_t a = 0; a < len; a++) { tail[a] = scratch[a].dst; w[a] = scratch[a].w; }
+}
+
+/* CSR sorted by (src, dst) from a triple list (distgraph.cpp:899-952 order):
+ * a counting sort by source, then each row sorted by destination. The
+ * generators never emit a (src, dst) pair twice, so the order is unique. */
+static int csr_from_triples(int64_t n, const vo_trip *t, int64_t m, vo_graph *out)
+{
     if (vo_graph_alloc(out, n, m)) return -1;
     for (int64_t k = 0; k < m; k++) out->rowptr[t[k].src + 1]++;
     for (int64_t i = 0; i < n; i++) out->rowptr[i + 1] += out->rowptr[i];
+    int64_t *fill = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+    if (!fill) return -1;
+    memcpy(fill, out->rowptr, sizeof(int64_t) * (size_t)n);
+    int64_t maxlen = 0;
     for (int64_t k = 0; k < m; k++) {
-        out->tail[k] = t[k].dst;
-        out->weight[k] = t[k].w;
+        const int64_t p = fill[t[k].src]++;
+        out->tail[p] = t[k].dst;
+        out->weight[p] = t[k].w;
     }
+    free(fill);
+    for (int64_t i = 0; i < n; i++) {
+        const int64_t len = out->rowptr[i + 1] - out->rowptr[i];
+        if (len > maxlen) maxlen = len;
+    }
+    vo_half *scratch = (vo_half *)malloc(sizeof(vo_half) * (size_t)(maxlen > 0 ? maxlen : 1));
+    if (!scratch) return -1;
+    for (int64_t i = 0; i < n; i++)
+        sort_row(out->tail + out->rowptr[i], out->weight + out->rowptr[i],
+                 out->rowptr[i + 1] - out->rowptr[i], scratch);
+    free(scratch);
     return 0;
+}
+
+/* 1 when row i of a (src, dst)-sorted CSR holds tail j (binary search). */
+static int csr_has(const vo_graph *g, int64_t i, int64_t j)
+{
+    int64_t lo = g->rowptr[i], hi = g->rowptr[i + 1];
+    while (lo < hi) {
+        const int64_t mid = lo + (hi - lo) / 2;
+        if (g->tail[mid] < j) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < g->rowptr[i + 1] && g->tail[lo] == j;
 }
 
 /* generateRGG for one rank (distgraph.cpp:412-983) without extra edges. The
@@ -190,7 +242,10 @@ int vo_rgg(int64_t n, vo_graph *out)
     }
     int64_t cap = 16 * n + 16, m = 0;
     vo_trip *t = (vo_trip *)malloc(sizeof(vo_trip) * (size_t)cap);
-    for (int64_t i = 0; i < n; i++) {
+    /* vertices visited cell by cell (neighbouring points stay in cache); the
+     * CSR assembly sorts the pairs, so the visiting order leaves it unchanged */
+    for (int64_t q = 0; q < n; q++) {
+        const int64_t i = order[q];
         const int64_t cx = cell[i] % ncx, cy = cell[i] / ncx;
         for (int64_t ny = cy - 1; ny <= cy + 1; ny++) {
             if (ny < 0 || ny >= ncy) continue;
@@ -266,10 +321,11 @@ int64_t vo_add_random_edges(const vo_graph *in, double percent, uint64_t seed, v
 {
     const int64_t n = in->nv, m0 = in->ne / 2;
     const int64_t nrande = ((int64_t)(percent * (double)m0)) / 100;
+    /* pairs already in the graph (either direction) are found by binary
+     * searches of the two rows, which are sorted by tail; the set holds only
+     * the candidates accepted so far */
     vo_set s;
-    set_init(&s, in->ne / 2 + nrande);
-    for (int64_t i = 0; i < n; i++)
-        for (int64_t e = in->rowptr[i]; e < in->rowptr[i + 1]; e++) set_insert(&s, pair_key(i, in->tail[e], n));
+    set_init(&s, nrande);
     int64_t m = in->ne;
     vo_trip *t = (vo_trip *)malloc(sizeof(vo_trip) * (size_t)(in->ne + 2 * nrande + 1));
     for (int64_t i = 0; i < n; i++)
@@ -281,6 +337,7 @@ int64_t vo_add_random_edges(const vo_graph *in, double percent, uint64_t seed, v
         const int64_t i = (int64_t)uint_below(vo_mix(seed, 1, (uint64_t)k), (uint64_t)n);
         const int64_t j = (int64_t)uint_below(vo_mix(seed, 2, (uint64_t)k), (uint64_t)n);
         if (i == j) continue;
+        if (csr_has(in, i, j) || csr_has(in, j, i)) continue;
         if (!set_insert(&s, pair_key(i, j, n))) continue;
         const double w = unit_double(vo_mix(seed, 3, (uint64_t)k));
         t[m].src = i; t[m].dst = j; t[m].w = w; m++;

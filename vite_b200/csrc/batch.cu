@@ -184,7 +184,56 @@ struct BJob {
     int64_t nv = 0, ne = 0;
 };
 
+// one graph's level map: all[i] = rank of the label of level-0 vertex i (or, at
+// level 0, of vertex i itself) among the labels in use at this level
+__global__ void k_compose_one(int32_t *__restrict__ all, int64_t n0, int32_t first,
+                              const int32_t *__restrict__ cvr, const int64_t *__restrict__ rank) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n0;
+         i += (int64_t)gridDim.x * blockDim.x)
+        all[i] = (int32_t)rank[cvr[first ? i : all[i]]];
+}
+
+__global__ void k_widen(const int32_t *__restrict__ x, int64_t n, int64_t *__restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = x[i];
+}
+
 } // namespace
+
+// main.cpp:381-425 for one graph on the device: the level's communities (in
+// reference numbering) are renamed by their rank among the labels in use, then
+// composed into the level-0 map `all` (n0 entries; at level 0 the renamed
+// labels themselves)
+void vg_compose_level(vg_ctx *ctx, const vg_graph *g, int32_t *all, int64_t n0, bool first) {
+    const int64_t n = g->nv;
+    if (!n || !n0) return;
+    const int grid = vg_grid(ctx, n, 256);
+    DevBuf<int32_t> cvr(ctx, n), used(ctx, n);
+    DevBuf<int64_t> rank(ctx, n);
+    VG_CUDA(cudaMemsetAsync(used.p, 0, sizeof(int32_t) * n, ctx->stream));
+    { LaunchTimer lt(ctx); k_comm_ref<<<grid, 256, 0, ctx->stream>>>(g->comm, g->ref, n, cvr.p); }
+    VG_CHECK_LAUNCH();
+    { LaunchTimer lt(ctx); k_mark_used<<<grid, 256, 0, ctx->stream>>>(cvr.p, n, used.p); }
+    VG_CHECK_LAUNCH();
+    vg_scan_i32_async(ctx, used.p, rank.p, n, nullptr);
+    { LaunchTimer lt(ctx);
+      k_compose_one<<<vg_grid(ctx, n0, 256), 256, 0, ctx->stream>>>(all, n0, first ? 1 : 0, cvr.p,
+                                                                    rank.p); }
+    VG_CHECK_LAUNCH();
+}
+
+// the level-0 map widened to Vite's 64-bit ids and copied to the host buffer
+// `out` (pinned memory makes the copy a single DMA at the link's rate)
+void vg_download_map(vg_ctx *ctx, const int32_t *all, int64_t n0, int64_t *out) {
+    if (!n0) return;
+    DevBuf<int64_t> wide(ctx, n0);
+    { LaunchTimer lt(ctx);
+      k_widen<<<vg_grid(ctx, n0, 256), 256, 0, ctx->stream>>>(all, n0, wide.p); }
+    VG_CHECK_LAUNCH();
+    VG_CUDA(cudaMemcpyAsync(out, wide.p, sizeof(int64_t) * n0, cudaMemcpyDeviceToHost, ctx->stream));
+    vg_sync(ctx);
+}
 
 struct vg_batch {
     vg_ctx *ctx = nullptr;

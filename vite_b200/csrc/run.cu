@@ -4,8 +4,6 @@
 // re-run under threshold cycling (:448-463) and the phase caps (:504-512).
 #include "vg_internal.cuh"
 
-#include <algorithm>
-#include <map>
 
 void vg_phase_internal(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double *mod_out,
                        int32_t *iters_out, double *sweep_ms, int64_t *edges);
@@ -35,23 +33,6 @@ struct EventTimer {
         if (b) cudaEventDestroy(b);
     }
 };
-
-// main.cpp:381-425: renumber the level's communities by sorted id and compose
-// with the previous levels' map (literally, as the reference does)
-void compose_output(std::vector<int64_t> &commAll, const std::vector<int64_t> &cvect, int phase) {
-    std::vector<int64_t> ren(cvect);
-    std::sort(ren.begin(), ren.end());
-    std::map<int64_t, int64_t> kval;
-    int64_t nidx = 0;
-    for (int64_t x : ren)
-        if (kval.find(x) == kval.end()) kval.emplace(x, nidx++);
-    std::vector<int64_t> all(cvect.size());
-    for (size_t c = 0; c < cvect.size(); c++) all[c] = kval[cvect[c]];
-    if (phase == 0)
-        std::copy(all.begin(), all.end(), commAll.begin());
-    else
-        for (size_t p = 0; p < commAll.size(); p++) commAll[p] = all[commAll[p]];
-}
 
 } // namespace
 
@@ -88,8 +69,9 @@ extern "C" vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g0, const vg_ru
             cur = owned;
             layout_s = tl.stop_ms() * 1e-3;
         }
-        std::vector<int64_t> commAll;
-        if (comm_out) commAll.assign(g0->nv, -1);
+        // the -o map lives on the device; it is copied out once at the end
+        DevBuf<int32_t> commAll;
+        if (comm_out) commAll.alloc(ctx, g0->nv);
         double currMod = -1.0, prevMod = -1.0, threshold = rp->threshold;
         int phase = 0, short_phase = 0, tot_iters = 0, nrec = 0;
         auto cleanup_view = [&] {
@@ -138,11 +120,7 @@ extern "C" vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g0, const vg_ru
                 tot_iters += iters;
                 const bool accepted = (currMod - prevMod) > threshold;
                 if (accepted) {
-                    if (comm_out) {
-                        std::vector<int64_t> cv(cur->nv);
-                        vg_download_comm_ref(ctx, cur, cur->comm, cv.data());
-                        compose_output(commAll, cv, phase);
-                    }
+                    if (comm_out) vg_compose_level(ctx, cur, commAll.p, g0->nv, phase == 0);
                     if (!rp->one_phase) {
                         EventTimer tr(ctx->stream);
                         vg_graph *next = vg_rebuild_new(ctx, cur, cur->comm);
@@ -192,7 +170,7 @@ extern "C" vg_status vg_louvain_run(vg_ctx *ctx, const vg_graph *g0, const vg_ru
         }
         cleanup_view();
         if (nlevels_out) *nlevels_out = nrec;
-        if (comm_out) std::copy(commAll.begin(), commAll.end(), comm_out);
+        if (comm_out) vg_download_map(ctx, commAll.p, g0->nv, comm_out);
         vg_sync(ctx);
     });
     if (owned) {

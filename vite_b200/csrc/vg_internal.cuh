@@ -148,6 +148,10 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order);
 vg_graph *vg_apply_layout(vg_ctx *ctx, const vg_graph *g, const int32_t *order);
 vg_graph *vg_remove_layout(vg_ctx *ctx, const vg_graph *g);
 void vg_download_comm_ref(vg_ctx *ctx, const vg_graph *g, const int32_t *comm, int64_t *out);
+// graphClustering's -o map (main.cpp:381-425) built on the device: compose level g's
+// communities into the level-0 map `all` (n0 int32 entries), then copy it out as int64
+void vg_compose_level(vg_ctx *ctx, const vg_graph *g, int32_t *all, int64_t n0, bool first);
+void vg_download_map(vg_ctx *ctx, const int32_t *all, int64_t n0, int64_t *out);
 void vg_download_vals_ref(vg_ctx *ctx, const vg_graph *g, const int32_t *x, int64_t *out);
 void vg_ref_to_pos_inplace(vg_ctx *ctx, const vg_graph *g, int32_t *x, bool are_ids);
 // whether the locality layout pays for g (sampled clustering coefficient)
