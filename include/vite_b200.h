@@ -133,6 +133,31 @@ vg_status vg_graph_free(vg_ctx *ctx, vg_graph *g);
 vg_status vg_graph_read_vite(vg_ctx *ctx, const char *path, vg_graph **out);
 vg_status vg_graph_write_vite(vg_ctx *ctx, const vg_graph *g, const char *path);
 
+/* Text edge lists parsed on the device into a graph: fileConvert's input formats and
+ * weight options (converters/convert.cpp:102-281, parseCommandLine :286-368), replacing
+ * loadSimpleFile (converters/simple.cpp:61), loadSNAPFile (converters/snap.cpp:65) and
+ * loadMatrixMarketFile (converters/matrix-market.cpp:65) followed by processGraphData
+ * (utils.cpp:101-152). Rows list their tails in increasing order (equal pairs in file
+ * order), duplicates kept. A malformed file is VG_ERR_ARG with the line named. */
+typedef enum vg_text_format {
+    VG_TEXT_SIMPLE = 1,        /* -s: "u v [w]" per line, '#'/'%' comment lines */
+    VG_TEXT_SNAP = 2,          /* -n: "# Nodes: N Edges: M" header, ids renumbered */
+    VG_TEXT_MATRIX_MARKET = 3  /* -m: coordinate, general or symmetric, 1-based */
+} vg_text_format;
+typedef enum vg_text_weights {
+    VG_WEIGHTS_ABS = 0,        /* default: |w| (pattern files and SNAP: 1) */
+    VG_WEIGHTS_ORIGINAL = 1,   /* -i: w as written */
+    VG_WEIGHTS_ONE = 2,        /* -w: 1 */
+    VG_WEIGHTS_RANDOM = 3      /* -r: the reference's genRandom stream (utils.cpp:93-99) */
+} vg_text_weights;
+typedef struct vg_text_params {
+    int32_t format;            /* vg_text_format */
+    int32_t weights;           /* vg_text_weights */
+    int32_t one_based;         /* -z: ids start at 1 (VG_TEXT_SIMPLE only) */
+} vg_text_params;
+vg_status vg_graph_read_text(vg_ctx *ctx, const char *path, const vg_text_params *p,
+                             vg_graph **out);
+
 /* Store the graph in another vertex order on the device (no reference
  * counterpart: the reference keeps its input order). mode 1: locality order
  * (multi-source BFS clusters) so that a sweep's gathers stay in few cache
@@ -152,14 +177,20 @@ vg_status vg_vertex_degree(vg_ctx *ctx, vg_graph *g, double *vdeg_out, double *c
  * on an allocation mid-run. The caller passes device pointers: rowptr int64[nv+1]
  * and weights f64[ne] of a CSR (weights may be NULL only when the CSR holds no
  * entries, else VG_ERR_ARG), and vdeg_out f64[nv] for the degrees; 1/(2m) is
- * written to *constant_out (host). Runs on `stream` (a cudaStream_t, NULL = default
- * stream) of the current device and returns after the stream has finished. The
- * scratch of the reduction is a file-scope device array of 512 KiB held by every GPU
- * that loads the library: at most VG_NOALLOC_MAX_VERTICES vertices, larger graphs
- * are rejected with VG_ERR_ARG. All calls share that array, so calls that overlap on
- * the GPU race. The first call on a device looks the array's address up with that
- * device current; make it before any stream capture. errbuf (may be NULL) receives a
- * message on failure. Allocates nothing: no cudaMalloc, no cudaFree. */
+ * written to *constant_out (host). The CSR must be valid: offsets non-decreasing and
+ * every offset in [0, ne] of the weights array the caller passes. Unlike
+ * vg_graph_upload, this function does not check the offsets (a check would need
+ * memory of its own); offsets past the weights array make the kernel read out of
+ * bounds. Runs on `stream` (a cudaStream_t, NULL = default stream) of the current
+ * device and waits for that stream to finish before it returns. The scratch of the
+ * reduction is a file-scope device array of 512 KiB held by every GPU that loads the
+ * library: at most VG_NOALLOC_MAX_VERTICES vertices, larger graphs are rejected with
+ * VG_ERR_ARG. All calls share that array, so calls that overlap on the GPU race. The
+ * first call on a device looks the array's address up with that device current; make
+ * it before any stream capture. The address is kept for the life of the process, so
+ * do not call this function again on a device after cudaDeviceReset. errbuf (may be
+ * NULL) receives a message on failure. Allocates nothing: no cudaMalloc, no
+ * cudaFree. */
 #define VG_NOALLOC_MAX_VERTICES (2048LL * 65536LL)
 vg_status vg_vertex_degree_noalloc(int64_t nv, const int64_t *d_rowptr, const double *d_weight,
                                    double *d_vdeg_out, double *constant_out, void *stream,

@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 HARNESS = os.path.join(REF_DIR, "vite_ref_harness")
+FILE_CONVERT = os.path.join(REF_DIR, "fileConvert")
 REF_MAIN = os.path.join(REF_DIR, "graphClustering")
 
 _i64p = C.POINTER(C.c_int64)
@@ -40,12 +41,24 @@ class _VoRun(C.Structure):
                 ("et_delta", C.c_double), ("threshold_scaling", C.c_int), ("one_phase", C.c_int)]
 
 
+def reference_dir() -> str:
+    """Directory of the reference sources: $VITE_REFERENCE_DIR when set, else the
+    default written in oracle/Makefile (the one place that names it)."""
+    d = os.environ.get("VITE_REFERENCE_DIR")
+    if d:
+        return d
+    res = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True,
+                         text=True)
+    return res.stdout.strip()
+
+
 def build(quiet: bool = True) -> None:
     """Compile liboracle.so (and, when the reference sources are present, oracle/_ref)."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "restate"], check=True, stdout=out)
-    if os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-C", HERE, "-j8", "ref"], check=True, stdout=out)
+    ref = reference_dir()
+    if ref and os.path.isdir(ref):
+        subprocess.run(["make", "-C", HERE, "-j8", f"REF={ref}", "ref"], check=True, stdout=out)
 
 
 _lib = None
@@ -341,12 +354,48 @@ def read_record(path: str) -> RefRecord:
     return rec
 
 
-def run_harness(args: list[str], record: str, threads: int = 1, timeout: float = 3600.0) -> str:
-    """Run the reference harness (oracle/_ref) and return its stdout."""
+def run_harness(args: list[str], record: str | None, threads: int = 1,
+                timeout: float = 3600.0) -> str:
+    """Run the reference harness (oracle/_ref) and return its stdout; `record` names the
+    record file of the first run (None: no record)."""
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
-    res = subprocess.run([HARNESS, *args, "-w", record], capture_output=True, text=True,
+    rec = ["-w", record] if record else []
+    res = subprocess.run([HARNESS, *args, *rec], capture_output=True, text=True,
                          env=env, timeout=timeout, check=True)
     return res.stdout
+
+
+def harness_totals(out: str) -> list[dict]:
+    """The per-run totals a harness run printed (one line per run of the level loop)."""
+    runs = []
+    for line in out.splitlines():
+        if line.startswith("HARNESS total_clustering_s"):
+            f = line.split()
+            runs.append({"clustering_s": float(f[2]), "rebuild_s": float(f[4]),
+                         "total_s": float(f[6]), "levels": int(f[8]), "iterations": int(f[10]),
+                         "final_mod": float(f[12])})
+    return runs
+
+
+def harness_read_seconds(out: str) -> float:
+    for line in out.splitlines():
+        if line.startswith("HARNESS graph_seconds"):
+            return float(line.split()[2])
+    return float("nan")
+
+
+def output_map(levels: list, threshold: float = 1e-6) -> np.ndarray:
+    """graphClustering's -o map (main.cpp:381-425) from a record's levels: every accepted
+    level's communities renamed by sorted rank, composed into the level-0 map."""
+    allmap = None
+    prev = -1.0
+    for lv in levels:
+        if lv.level < 0 or not (lv.mod - prev) > threshold:
+            break
+        _, inv = np.unique(lv.cvect, return_inverse=True)
+        allmap = inv.astype(np.int64) if allmap is None else inv[allmap].astype(np.int64)
+        prev = lv.mod
+    return allmap
 
 
 @dataclass
@@ -457,3 +506,215 @@ def golden_graph(entry: dict) -> Graph:
     if kind == "rggx":
         return add_random_edges(rgg(int(rest[0])), float(rest[1]), int(rest[2]))[0]
     raise ValueError(src)
+
+
+# --------------------------------------------------------------------------------------
+# fileConvert's text readers (converters/convert.cpp:102-281): plain edge lists (-s,
+# converters/simple.cpp:61-160), SNAP (-n, converters/snap.cpp:65-196) and Matrix Market
+# (-m, converters/matrix-market.cpp:65-241), then processGraphData (utils.cpp:101-152)
+
+import re as _re
+
+_I64 = _re.compile(rb"[ \t\r\v\f]*([+-]?[0-9]+)")
+_F64 = _re.compile(rb"[ \t\r\v\f]*([+-]?(?:[0-9]+\.?[0-9]*|\.[0-9]+)(?:[eE][+-]?[0-9]+)?)")
+
+
+def _read_i64(line: bytes, pos: int):
+    """operator>>(long long&) from pos: (value, new pos) or None."""
+    m = _I64.match(line, pos)
+    if not m:
+        return None
+    v = int(m.group(1))
+    if not -(1 << 63) <= v < (1 << 63):
+        return None
+    return v, m.end()
+
+
+def _read_f64(line: bytes, pos: int):
+    """operator>>(double&): the correctly rounded value, or 0.0 when no number starts
+    here (C++11 stores 0 on a failed read)."""
+    m = _F64.match(line, pos)
+    return float(m.group(1)) if m else 0.0
+
+
+class _GenRandom:
+    """genRandom(0.01, 1.0)'s stream, one weight per call (see gen_random_weights)."""
+
+    def __init__(self):
+        self.x = 1
+
+    def __call__(self) -> float:
+        M = 2147483647
+        self.x = (self.x * 16807) % M
+        x1 = self.x
+        self.x = (self.x * 16807) % M
+        x2 = self.x
+        s = float(x1 - 1) * 1.0
+        s = s + float(x2 - 1) * 2147483646.0
+        c = s / float(2147483646 * 2147483646)
+        if c >= 1.0:
+            c = float(np.nextafter(1.0, 0.0))
+        return c * (1.0 - 0.01) + 0.01
+
+
+def gen_random_weights(count: int) -> np.ndarray:
+    """genRandom(0.01, 1.0) (utils.cpp:93-99) called `count` times: a static
+    std::default_random_engine (minstd_rand0, x <- 16807 x mod 2^31 - 1, seed 1) through
+    std::uniform_real_distribution<double>, whose generate_canonical<double, 53> takes
+    two draws (range r = 2^31 - 2): c = ((x1 - 1) + (x2 - 1) * r) / r^2, then
+    0.01 + c * (1.0 - 0.01); restated from the C++ standard's definitions."""
+    out = np.empty(count, dtype=np.float64)
+    x = 1
+    M = 2147483647
+    r = 2147483646.0
+    rr = float(2147483646 * 2147483646)
+    for k in range(count):
+        x = (x * 16807) % M
+        x1 = x
+        x = (x * 16807) % M
+        x2 = x
+        s = float(x1 - 1) * 1.0
+        s = s + float(x2 - 1) * r
+        c = s / rr
+        if c >= 1.0:
+            c = np.nextafter(1.0, 0.0)
+        out[k] = c * (1.0 - 0.01) + 0.01
+    return out
+
+
+def _csr_from_list(nv: int, src, dst, w) -> Graph:
+    """processGraphData: counts per source, entries sorted by (source, tail); equal pairs
+    keep their list order (std::sort leaves them unspecified)."""
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    w = np.asarray(w, dtype=np.float64)
+    order = np.lexsort((dst, src)) if len(src) else np.zeros(0, np.int64)
+    rp = np.zeros(nv + 1, dtype=np.int64)
+    if len(src):
+        np.add.at(rp, src + 1, 1)
+    rp = np.cumsum(rp)
+    return Graph(rp, dst[order], w[order])
+
+
+def canonical_ties(g: Graph) -> np.ndarray:
+    """The weights with every run of equal (row, tail) entries sorted by weight bits:
+    std::sort leaves such runs in an unspecified order, so comparisons with the
+    reference's converter output go through this."""
+    rows = np.repeat(np.arange(g.nv, dtype=np.int64), np.diff(g.rowptr))
+    order = np.lexsort((g.weight.view(np.int64), g.tail, rows))
+    return g.weight[order]
+
+
+def read_text(path: str, fmt: str, weights: str = "abs", one_based: bool = False) -> Graph:
+    """fileConvert -s/-n/-m [-w|-i|-r] [-z] as a Graph. fmt: 'simple', 'snap' or 'mm';
+    weights: 'abs' (default), 'orig' (-i), 'one' (-w), 'random' (-r)."""
+    data = open(path, "rb").read()
+    src, dst, w = [], [], []
+    rnd = _GenRandom()
+
+    def weight_of(x: float) -> float:
+        if weights == "one":
+            return 1.0
+        if weights == "random":
+            return rnd()
+        return abs(x) if weights == "abs" else x
+
+    if fmt == "simple":
+        pieces = data.split(b"\n")  # the last piece is the text after the last newline
+        read_w = weights in ("abs", "orig")
+        mx = -1
+        for k, line in enumerate(pieces):  # first pass: the largest id (simple.cpp:78-102)
+            if line[:1] in (b"#", b"%"):
+                continue
+            a = _read_i64(line, 0)
+            if a is None:
+                v0 = 0 - (1 if one_based else 0)
+                mx = max(mx, v0)
+                continue
+            b = _read_i64(line, a[1])
+            v0 = a[0] - (1 if one_based else 0)
+            v1 = b[0] - (1 if one_based else 0) if b else v0
+            mx = max(mx, v0, v1)
+        nv = mx + 1
+        for k, line in enumerate(pieces[:-1]):  # second pass: every piece but the last
+            if line[:1] in (b"#", b"%"):
+                continue
+            a = _read_i64(line, 0)
+            b = _read_i64(line, a[1]) if a else None
+            if a is None or b is None:
+                raise ValueError(f"line {k + 1}: two ids expected")
+            x = _read_f64(line, b[1]) if read_w else 0.0
+            v0, v1 = a[0], b[0]
+            if one_based:
+                v0, v1 = v0 - 1, v1 - 1
+            x = weight_of(x)
+            src += [v0, v1]
+            dst += [v1, v0]
+            w += [x, x]
+        return _csr_from_list(nv, src, dst, w)
+
+    if fmt == "snap":
+        pos = 0
+        nv = ne = None
+        lines = data.split(b"\n")
+        i = 0
+        while i < len(lines) and lines[i][:1] == b"#":
+            line = lines[i].decode()
+            if "Nodes" in line:
+                nums = [int(_re.match(r"\s*([+-]?\d+)", part).group(1))
+                        for part in line.split(":")[1:3]]
+                nv, ne = nums
+            pos += len(lines[i]) + 1
+            i += 1
+        toks = data[pos:].split()[: 2 * ne]
+        if len(toks) < 2 * ne:
+            raise ValueError("fewer ids than the header's edges")
+        newid: dict = {}
+        ids = []
+        for t in toks:
+            v = int(t)
+            if v not in newid:
+                newid[v] = len(newid)
+            ids.append(newid[v])
+        for k in range(ne):
+            x = weight_of(1.0) if weights == "random" else 1.0
+            u, v = ids[2 * k], ids[2 * k + 1]
+            src += [u, v]
+            dst += [v, u]
+            w += [x, x]
+        return _csr_from_list(nv, src, dst, w)
+
+    if fmt == "mm":
+        lines = data.split(b"\n")
+        banner = lines[0].split()
+        field, symm = banner[3].upper(), banner[4].upper()
+        pattern = field == b"PATTERN"
+        symmetric = symm == b"SYMMETRIC"
+        i = 1
+        while lines[i][:1] == b"%":
+            i += 1
+        ns, _, ne = (int(x) for x in lines[i].split()[:3])
+        nv = ns
+        read_w = not pattern and weights in ("abs", "orig")
+        for k in range(ne):
+            line = lines[i + 1 + k]
+            a = _read_i64(line, 0)
+            b = _read_i64(line, a[1])
+            x = _read_f64(line, b[1]) if read_w else 1.0
+            if weights == "abs" and not pattern:
+                x = abs(x)
+            if weights == "one":
+                x = 1.0
+            if weights == "random":
+                x = weight_of(1.0)
+            s, d = a[0] - 1, b[0] - 1
+            if symmetric and s != d:
+                src += [s, d]
+                dst += [d, s]
+                w += [x, x]
+            else:
+                src.append(s)
+                dst.append(d)
+                w.append(x)
+        return _csr_from_list(nv, src, dst, w)
+    raise ValueError(fmt)

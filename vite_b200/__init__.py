@@ -38,8 +38,12 @@ EXPORTED_SYMBOLS = [
     "vg_batch_create", "vg_batch_destroy", "vg_batch_submit", "vg_batch_step", "vg_batch_poll",
     "vg_batch_result", "vg_batch_forget", "vg_batch_get_stats", "vg_compare_communities",
     "vg_ctx_get_tuning", "vg_ctx_set_tuning", "vg_autotune",
-    "vg_graph_read_vite", "vg_graph_write_vite",
+    "vg_graph_read_vite", "vg_graph_write_vite", "vg_graph_read_text",
 ]
+
+# vg_text_format / vg_text_weights (fileConvert's -s/-n/-m and -w/-i/-r)
+TEXT_FORMATS = {"simple": 1, "snap": 2, "mm": 3}
+TEXT_WEIGHTS = {"abs": 0, "orig": 1, "one": 2, "random": 3}
 
 VG_BATCH_TAKE = 1
 VG_BATCH_COMM = 2
@@ -83,6 +87,10 @@ class CompareStats(C.Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class TextParams(C.Structure):
+    _fields_ = [("format", C.c_int32), ("weights", C.c_int32), ("one_based", C.c_int32)]
 
 
 class Tuning(C.Structure):
@@ -162,6 +170,7 @@ def lib() -> C.CDLL:
         L.vg_compare_communities.argtypes = [vp, C.c_int64, _i64p, _i64p, C.POINTER(CompareStats)]
         L.vg_graph_read_vite.argtypes = [vp, C.c_char_p, C.POINTER(vp)]
         L.vg_graph_write_vite.argtypes = [vp, vp, C.c_char_p]
+        L.vg_graph_read_text.argtypes = [vp, C.c_char_p, C.POINTER(TextParams), C.POINTER(vp)]
         L.vg_ctx_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.vg_ctx_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.vg_autotune.argtypes = [vp, C.POINTER(vp), C.c_int32, C.c_int32, C.POINTER(Tuning),
@@ -375,13 +384,22 @@ class Context:
             vertex_order: bool = False, max_colors: int = 8, single_color_iter: bool = False,
             et_type: int = 0, et_delta: float = 1.0, threshold_scaling: bool = False,
             one_phase: bool = False, want_comm: bool = False, max_levels: int = 256,
-            layout: int = 2) -> Levels:
+            layout: int = 2, comm_out: np.ndarray | None = None) -> Levels:
+        """graphClustering's phase loop (vg_louvain_run). With want_comm, or a caller's
+        int64 buffer `comm_out` of nv entries (pinned memory copies fastest), the -o map
+        of level-0 vertices to final communities is returned as Levels.comm."""
         p = RunParams(threshold, int(coloring), int(vertex_order), max_colors,
                       int(single_color_iter), et_type, et_delta, int(threshold_scaling),
                       int(one_phase), layout)
         stats = (LevelStat * max_levels)()
         n = C.c_int32()
-        comm = np.empty(g.nv, np.int64) if want_comm else None
+        if comm_out is not None:
+            if (comm_out.dtype != np.int64 or comm_out.shape != (g.nv,)
+                    or not comm_out.flags.c_contiguous):
+                raise VgError(VG_ERR_ARG, "comm_out must be a contiguous int64 array of nv entries")
+            comm = comm_out
+        else:
+            comm = np.empty(g.nv, np.int64) if want_comm else None
         self._check(lib().vg_louvain_run(self.handle, g.handle, C.byref(p), stats, max_levels,
                                          C.byref(n), _ptr(comm)))
         return Levels([stats[i].as_dict() for i in range(min(n.value, max_levels))], comm)
@@ -402,6 +420,17 @@ class Context:
         """A Vite binary graph file straight into a device graph (vg_graph_read_vite)."""
         h = C.c_void_p()
         self._check(lib().vg_graph_read_vite(self.handle, os.fsencode(path), C.byref(h)))
+        return Graph(self, h)
+
+    def read_text(self, path: str, fmt: str, weights: str = "abs",
+                  one_based: bool = False) -> Graph:
+        """A text edge list parsed on the device (vg_graph_read_text): fmt 'simple' (-s),
+        'snap' (-n) or 'mm' (-m); weights 'abs' (default), 'orig' (-i), 'one' (-w),
+        'random' (-r); one_based is -z."""
+        p = TextParams(TEXT_FORMATS[fmt], TEXT_WEIGHTS[weights], int(one_based))
+        h = C.c_void_p()
+        self._check(lib().vg_graph_read_text(self.handle, os.fsencode(path), C.byref(p),
+                                             C.byref(h)))
         return Graph(self, h)
 
     def write_vite(self, g: Graph, path: str) -> None:
