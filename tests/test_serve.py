@@ -41,3 +41,34 @@ def test_served_results_equal_alone(ctx, lanes):
         assert [x["modularity"] for x in r.levels] == [x["modularity"] for x in a.stats]
     for g in gs:
         g.free()
+
+
+def test_host_requests_uploaded_on_admission(ctx):
+    """Requests held in host memory (Vite's CSR) are uploaded when admitted; with a
+    budget that admits about two graphs at a time the others wait, and every result is
+    still the one the graph gets alone."""
+    import vite_b200
+
+    start = ctx.bytes_in_use
+    reqs, alone = [], []
+    for k in range(8):
+        g = ctx.generate_rgg(2000 + 700 * k, 0.0, 0) if k % 2 == 0 else \
+            ctx.generate_ba(1500 + 400 * k, 4, 300 + k)
+        ctx.reweight(g, 1)
+        rp, tail, w = g.download()
+        ed = np.empty(len(tail), vite_b200.EDGE_DTYPE)
+        ed["tail"] = tail
+        ed["weight"] = w
+        alone.append(ctx.run(g, want_comm=True))
+        g.free()
+        reqs.append(sv.Request(None, arrival=0.001 * k, want_comm=True, rowptr=rp, edges=ed))
+    budget = 2 * max(r.footprint() for r in reqs)
+    rep = sv.serve(ctx, reqs, budget=budget)
+    for r, a in zip(rep.results, alone):
+        assert [(x["nv"], x["ne"], x["iters"], x["modularity"]) for x in r.levels] == \
+               [(x["nv"], x["ne"], x["iters"], x["modularity"]) for x in a.stats]
+        assert np.array_equal(r.comm, a.comm)
+    seq = sv.sequential(ctx, reqs)
+    for r, a in zip(seq.results, alone):
+        assert [x["modularity"] for x in r.levels] == [x["modularity"] for x in a.stats]
+    assert ctx.bytes_in_use == start  # every uploaded graph was released

@@ -102,6 +102,9 @@ struct SweepArgs {
     double *__restrict__ frozen;
     const uint8_t *__restrict__ active; // nullptr when early termination is off
     const int32_t *__restrict__ ref;     // reference id of each position (null: identity)
+    // set on the device when some vertex degree or non-empty community's degree is
+    // negative or NaN (then candidate pruning is off); null: pruning off
+    const int32_t *__restrict__ noprune;
     int64_t ne;                          // CSR entries (bounds of the vector loads)
     double constant;
     // batched graphs (null for one graph): the graph of each vertex, each graph's
@@ -136,6 +139,236 @@ __device__ __forceinline__ bool better(bool ok_a, double g_a, int32_t c_a, bool 
     if (!ok_a) return false;
     if (!ok_b) return true;
     return g_a > g_b || (g_a == g_b && vg_rid(ref, c_a) < vg_rid(ref, c_b));
+}
+
+// Candidate pruning (exact). With vd >= 0, a finite constant >= 0 and every
+// candidate community's degree ay >= 0 (*noprune == 0), gain_of(eiy, eix, vd, 0, ax,
+// constant) is an upper bound of the computed gain for every such ay: each rounding
+// step of gain_of is monotone, a larger ay gives a larger (ay - ax), a larger second
+// term and a smaller difference. A candidate whose bound is below the best gain found
+// so far cannot win (nor tie), so its community degree is never read.
+__device__ __forceinline__ bool can_prune(const SweepArgs &a, double vd, double cst) {
+    return a.noprune && !__ldg(a.noprune) && vd >= 0.0 && isfinite(vd) && cst >= 0.0 &&
+           isfinite(cst);
+}
+
+// distGetMaxIndex (louvain.cpp:2220-2279) over one row of a one-thread kernel: the
+// communities c[j] whose bit is set in `first` (first occurrences in the row, all
+// below dmax), their counters at cnt[j * stride]. With pruning, everything in the
+// bound but the counter is fixed for the row and the bound is monotone in it, so the
+// two largest counters give the two largest bounds: the candidate with the largest
+// is evaluated first and the others only when their bound reaches the best gain
+// (the second-largest bound tells when none can). Without pruning, or when the two
+// largest bounds are equal (integral weights give many equal counters, and every
+// tied candidate must be read anyway), every candidate, eight community-degree loads
+// at a time.
+template <int T>
+__device__ __forceinline__ void best_of_row(const SweepArgs &a, const int32_t (&c)[T],
+                                            uint32_t first, int32_t cc, const double *cnt,
+                                            int stride, double eix, double vd, double ax,
+                                            double cst, int dmax, bool &ok, double &bg,
+                                            int32_t &bc) {
+    ok = false;
+    bg = 0.0;
+    bc = INT_MAX;
+    if (can_prune(a, vd, cst)) {
+        double e1 = -INFINITY, e2 = -INFINITY;
+        int32_t uc = -1;
+#pragma unroll
+        for (int j = 0; j < T; j++) {
+            if (j >= dmax) break;
+            if (((first >> j) & 1u) && c[j] != cc) {
+                const double w = cnt[j * stride];
+                if (w > e1) {
+                    e2 = e1;
+                    e1 = w;
+                    uc = c[j];
+                } else if (w > e2) {
+                    e2 = w;
+                }
+            }
+        }
+        if (uc < 0) return;
+        const double ub = gain_of(e1, eix, vd, 0.0, ax, cst);
+        if (!(ub > 0.0)) return; // no candidate has a positive bound: no move
+        const double u2 = e2 == -INFINITY ? -INFINITY : gain_of(e2, eix, vd, 0.0, ax, cst);
+        if (u2 < ub) {
+            const double g = gain_of(e1, eix, vd, __ldg(a.cdeg + uc), ax, cst);
+            if (g > 0.0) {
+                ok = true;
+                bg = g;
+                bc = uc;
+            }
+            if (!(u2 > 0.0 && (!ok || u2 >= bg))) return; // no other candidate can win
+#pragma unroll
+            for (int j = 0; j < T; j++) {
+                if (j >= dmax) break;
+                if (((first >> j) & 1u) && c[j] != cc && c[j] != uc) {
+                    const double w = cnt[j * stride];
+                    const double u = gain_of(w, eix, vd, 0.0, ax, cst);
+                    if (u > 0.0 && (!ok || u >= bg)) {
+                        const double g2 = gain_of(w, eix, vd, __ldg(a.cdeg + c[j]), ax, cst);
+                        if (g2 > 0.0 && better(true, g2, c[j], ok, bg, bc, a.ref)) {
+                            bg = g2;
+                            bc = c[j];
+                            ok = true;
+                        }
+                    }
+                }
+            }
+            return;
+        }
+        // a tie at the top: one round over every candidate below
+    }
+#pragma unroll
+    for (int b = 0; b < T; b += 8) {
+        if (b >= dmax) break;
+        double ay[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int j = b + q;
+            ay[q] = 0.0;
+            if (j < T && ((first >> j) & 1u) && c[j] != cc) ay[q] = __ldg(a.cdeg + c[j]);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int j = b + q;
+            if (j < T && ((first >> j) & 1u) && c[j] != cc) {
+                const double g = gain_of(cnt[j * stride], eix, vd, ay[q], ax, cst);
+                if (g > 0.0 && better(true, g, c[j], ok, bg, bc, a.ref)) {
+                    bg = g;
+                    bc = c[j];
+                    ok = true;
+                }
+            }
+        }
+    }
+}
+
+// distGetMaxIndex over the candidate slots keys/vals[i], i = base + lane + k * step < nk,
+// of one warp (all lanes call it); every lane returns the warp's best (ok, gain, cand).
+// With pruning (can_prune) the slot of largest bound is evaluated first and the others
+// only when their bound reaches the best gain; without, or when the largest bound is
+// shared by two slots, every slot, four community-degree loads per lane at a time. The
+// (gain, id) order makes the result independent of the visiting order.
+__device__ __forceinline__ void warp_best(const SweepArgs &a, const int32_t *keys,
+                                          const double *vals, int64_t base, int64_t step,
+                                          int64_t nk, double eix, double vd, double ax, double cst,
+                                          bool &ok, double &gain, int32_t &cand) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    ok = false;
+    gain = 0.0;
+    cand = INT_MAX;
+    bool scan_all = true;
+    if (can_prune(a, vd, cst)) { // vd and cst are the same in every lane
+        scan_all = false;
+        double ub = 0.0, u2 = 0.0, uw = 0.0;
+        int32_t uc = -1;
+        for (int64_t i = base + lane; i < nk; i += step) {
+            const double w = vals[i];
+            const double u = gain_of(w, eix, vd, 0.0, ax, cst);
+            if (u > ub) {
+                u2 = ub;
+                ub = u;
+                uc = keys[i];
+                uw = w;
+            } else if (u > u2) {
+                u2 = u;
+            }
+        }
+        double m = ub;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(full, m, o));
+        if (m > 0.0) {
+            const int wl = __ffs(__ballot_sync(full, uc >= 0 && ub == m)) - 1;
+            double sec = lane == wl ? u2 : ub; // the warp's second-largest bound
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sec = fmax(sec, __shfl_xor_sync(full, sec, o));
+            if (sec == m) {
+                // a tie at the top (integral weights): one round over every slot
+                scan_all = true;
+                goto full_scan;
+            }
+            double g = 0.0;
+            if (lane == wl) g = gain_of(uw, eix, vd, __ldg(a.cdeg + uc), ax, cst);
+            g = __shfl_sync(full, g, wl);
+            const int32_t c0 = __shfl_sync(full, uc, wl);
+            if (g > 0.0) {
+                ok = true;
+                gain = g;
+                cand = c0;
+            }
+            if (sec > 0.0 && (!ok || sec >= gain)) {
+                for (int64_t i = base + lane; i < nk; i += step) {
+                    const int32_t k = keys[i];
+                    if (k == c0) continue;
+                    const double w = vals[i];
+                    const double u = gain_of(w, eix, vd, 0.0, ax, cst);
+                    if (u > 0.0 && (!ok || u >= gain)) {
+                        const double gg = gain_of(w, eix, vd, __ldg(a.cdeg + k), ax, cst);
+                        if (gg > 0.0 && better(true, gg, k, ok, gain, cand, a.ref)) {
+                            gain = gg;
+                            cand = k;
+                            ok = true;
+                        }
+                    }
+                }
+                scan_all = false;
+            } else {
+                return; // every lane holds the warp's result
+            }
+        } else {
+            return; // no candidate has a positive bound: no move
+        }
+    }
+full_scan:
+    if (scan_all) {
+        for (int64_t i0 = base; i0 < nk; i0 += 4 * step) {
+            int32_t kq[4];
+            double aq[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int64_t i = i0 + j * step + lane;
+                kq[j] = i < nk ? keys[i] : EMPTY;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) aq[j] = kq[j] != EMPTY ? __ldg(a.cdeg + kq[j]) : 0.0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (kq[j] == EMPTY) continue;
+                const double g = gain_of(vals[i0 + j * step + lane], eix, vd, aq[j], ax, cst);
+                if (g > 0.0 && better(true, g, kq[j], ok, gain, cand, a.ref)) {
+                    gain = g;
+                    cand = kq[j];
+                    ok = true;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double og = __shfl_xor_sync(full, gain, o);
+        const int32_t oc = __shfl_xor_sync(full, cand, o);
+        const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
+        if (better(ook, og, oc, ok, gain, cand, a.ref)) {
+            gain = og;
+            cand = oc;
+            ok = true;
+        }
+    }
+}
+
+// the community sizes the singleton rule (louvain.cpp:2275-2276) reads: needed only
+// when the chosen community's id is larger than the current one's
+__device__ __forceinline__ void sizes_for_rule(const SweepArgs &a, bool ok, int32_t cand, int32_t cc,
+                                               int32_t &ccSize, int32_t &csz) {
+    ccSize = 0;
+    csz = 0;
+    if (ok && vg_rid(a.ref, cand) > vg_rid(a.ref, cc)) {
+        ccSize = __ldg(a.csize + cc);
+        csz = __ldg(a.csize + cand);
+    }
 }
 
 // decision + bookkeeping shared by all kernels (louvain.cpp:2275-2416)
@@ -263,31 +496,10 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? VG_T16_MINB : VG_T32_MINB)) k_s
             if (((first >> j) & 1u) && c[j] == cc) counter0 = ssum[j][tid];
         const double eix = __dsub_rn(counter0, selfLoop);
         const double ax = __dsub_rn(ccDeg, vd);
-        double bg = 0.0;
-        int32_t bc = INT_MAX;
-        bool ok = false;
-#pragma unroll
-        for (int b = 0; b < T; b += 8) {
-            double ay[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const int j = b + q;
-                ay[q] = 0.0;
-                if (((first >> j) & 1u) && c[j] != cc) ay[q] = __ldg(a.cdeg + c[j]);
-            }
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const int j = b + q;
-                if (((first >> j) & 1u) && c[j] != cc) {
-                    const double g = gain_of(ssum[j][tid], eix, vd, ay[q], ax, cst);
-                    if (g > 0.0 && better(true, g, c[j], ok, bg, bc, a.ref)) {
-                        bg = g;
-                        bc = c[j];
-                        ok = true;
-                    }
-                }
-            }
-        }
+        double bg;
+        int32_t bc;
+        bool ok;
+        best_of_row<T>(a, c, first, cc, &ssum[0][tid], NT, eix, vd, ax, cst, T, ok, bg, bc);
         // the singleton rule (louvain.cpp:2275-2276) needs the sizes only when
         // the winner's id is larger than the current community's
         int32_t ccSize = 0, bs = 0;
@@ -302,68 +514,59 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? VG_T16_MINB : VG_T32_MINB)) k_s
 // one vertex of a tile (degree d <= T): counters fold in place in the staged
 // weights of its row, in CSR order, at the slot of each community's first occurrence
 template <int T>
-__device__ __forceinline__ void tile_vertex(const SweepArgs &a, int32_t v, int d, double cst,
-                                            const int32_t *ts, double *ws) {
+__device__ __forceinline__ void tile_vertex(const SweepArgs &a, int32_t v, int d, int dmax,
+                                            double cst, const int32_t *ts, double *ws, int32_t cc,
+                                            double vd, double ccDeg) {
     if (a.active && !a.active[v]) {
         a.cw[v] = a.frozen[v];
         return;
     }
-    const int32_t cc = __ldg(a.curr + v);
-    const double vd = a.vdeg[v];
-    const double ccDeg = __ldg(a.cdeg + cc);
+    // every loop stops at dmax, the warp's largest degree (the same in every lane)
     int32_t c[T];
-    double selfLoop = 0.0;
+    uint32_t selfm = 0; // bit j: edge j is a self loop
 #pragma unroll
     for (int j = 0; j < T; j++) {
+        if (j >= dmax) break;
         c[j] = -1;
-        if (j < d) c[j] = __ldg(a.curr + ts[j]);
+        if (j < d) {
+            const int32_t t = ts[j];
+            c[j] = __ldg(a.curr + t);
+            if (t == v) selfm |= 1u << j;
+        }
     }
+    double selfLoop = 0.0;
+    if (selfm) {
 #pragma unroll
-    for (int j = 0; j < T; j++)
-        if (j < d && ts[j] == v) selfLoop = __dadd_rn(selfLoop, ws[j]);
+        for (int j = 0; j < T; j++) {
+            if (j >= dmax) break;
+            if ((selfm >> j) & 1u) selfLoop = __dadd_rn(selfLoop, ws[j]);
+        }
+    }
     uint32_t first = 0;
+    int j0 = -1; // first occurrence of the current community
 #pragma unroll
     for (int j = 0; j < T; j++) {
+        if (j >= dmax) break;
         if (j < d) {
             int fj = j;
 #pragma unroll
             for (int k = j - 1; k >= 0; k--)
                 if (c[k] == c[j]) fj = k;
-            if (fj == j) first |= 1u << j;
-            else ws[fj] = __dadd_rn(ws[fj], ws[j]);
-        }
-    }
-    double counter0 = 0.0;
-#pragma unroll
-    for (int j = 0; j < T; j++)
-        if (((first >> j) & 1u) && c[j] == cc) counter0 = ws[j];
-    const double eix = __dsub_rn(counter0, selfLoop);
-    const double ax = __dsub_rn(ccDeg, vd);
-    double bg = 0.0;
-    int32_t bc = INT_MAX;
-    bool ok = false;
-#pragma unroll
-    for (int b = 0; b < T; b += 8) {
-        double ay[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const int j = b + q;
-            ay[q] = 0.0;
-            if (j < T && ((first >> j) & 1u) && c[j] != cc) ay[q] = __ldg(a.cdeg + c[j]);
-        }
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const int j = b + q;
-            if (j < T && ((first >> j) & 1u) && c[j] != cc) {
-                const double g = gain_of(ws[j], eix, vd, ay[q], ax, cst);
-                if (g > 0.0 && better(true, g, c[j], ok, bg, bc, a.ref)) {
-                    bg = g;
-                    bc = c[j];
-                    ok = true;
-                }
+            if (fj == j) {
+                first |= 1u << j;
+                if (c[j] == cc) j0 = j;
+            } else {
+                ws[fj] = __dadd_rn(ws[fj], ws[j]);
             }
         }
     }
+    const double counter0 = j0 >= 0 ? ws[j0] : 0.0;
+    const double eix = __dsub_rn(counter0, selfLoop);
+    const double ax = __dsub_rn(ccDeg, vd);
+    double bg;
+    int32_t bc;
+    bool ok;
+    best_of_row<T>(a, c, first, cc, ws, 1, eix, vd, ax, cst, dmax, ok, bg, bc);
     int32_t ccSize = 0, bs = 0;
     if (ok && vg_rid(a.ref, bc) > vg_rid(a.ref, cc)) {
         ccSize = __ldg(a.csize + cc);
@@ -453,9 +656,19 @@ __global__ void __launch_bounds__(TILE_WARPS * 32, VG_TILE_MINB) k_sweep_tile(Sw
             off_t = lane * T;
             off_w = lane * T;
         }
+        // the vertex's own community, degree and community degree do not depend on
+        // the staged row: their loads overlap the staging copies
+        int32_t cc = 0;
+        double vd = 0.0, ccDeg = 0.0;
+        if (live && d <= T) {
+            cc = __ldg(a.curr + v);
+            vd = a.vdeg[v];
+            ccDeg = __ldg(a.cdeg + cc);
+        }
+        const int dmax = (int)__reduce_max_sync(0xffffffffu, (live && d <= T) ? (unsigned)d : 0u);
         cp_async_wait_all();
         __syncwarp();
-        if (live && d <= T) tile_vertex<T>(a, v, d, cst, st + off_t, sw + off_w);
+        if (live && d <= T) tile_vertex<T>(a, v, d, dmax, cst, st + off_t, sw + off_w, cc, vd, ccDeg);
         __syncwarp();
     }
 }
@@ -595,56 +808,18 @@ __global__ void __launch_bounds__(WARPS * 32, CAP <= 256 ? 4 : 1) k_sweep_warp(
             __syncwarp();
         }
         const double vd = a.vdeg[v];
-        double ccDeg;
-        int32_t ccSize;
-        load_comm(a, cc, ccDeg, ccSize);
+        const double ccDeg = __ldg(a.cdeg + cc);
         const double eix = __dsub_rn(counter0, selfLoop);
         const double ax = __dsub_rn(ccDeg, vd);
-        double gain = 0.0;
-        int32_t cand = INT_MAX, csz = 0;
-        bool ok = false;
-        // four candidates per lane per round, their community loads issued together;
-        // the (gain, id) order makes the winner independent of the visiting order
-        for (int i0 = 0; i0 < nk; i0 += 4 * 32) {
-            int32_t kq[4], sq[4];
-            double aq[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int i = i0 + j * 32 + lane;
-                kq[j] = i < nk ? keys[i] : EMPTY;
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                aq[j] = 0.0;
-                sq[j] = 0;
-                if (kq[j] != EMPTY) load_comm(a, kq[j], aq[j], sq[j]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                if (kq[j] == EMPTY) continue;
-                const double g = gain_of(vals[i0 + j * 32 + lane], eix, vd, aq[j], ax, cst);
-                if (g > 0.0 && better(true, g, kq[j], ok, gain, cand, a.ref)) {
-                    gain = g;
-                    cand = kq[j];
-                    csz = sq[j];
-                    ok = true;
-                }
-            }
+        double gain;
+        int32_t cand;
+        bool ok;
+        warp_best(a, keys, vals, 0, 32, nk, eix, vd, ax, cst, ok, gain, cand);
+        if (lane == 0) {
+            int32_t ccSize, csz;
+            sizes_for_rule(a, ok, cand, cc, ccSize, csz);
+            commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, cand, csz);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double og = __shfl_xor_sync(full, gain, o);
-            const int32_t oc = __shfl_xor_sync(full, cand, o);
-            const int32_t os = __shfl_xor_sync(full, csz, o);
-            const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
-            if (better(ook, og, oc, ok, gain, cand, a.ref)) {
-                gain = og;
-                cand = oc;
-                csz = os;
-                ok = true;
-            }
-        }
-        if (lane == 0) commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, cand, csz);
         __syncwarp();
     }
 }
@@ -658,7 +833,6 @@ __global__ void __launch_bounds__(WARPS * 32, CAP <= 256 ? 4 : 1) k_sweep_warp(
 struct CtaShared {
     double red_g[CT_THREADS / 32];
     int32_t red_c[CT_THREADS / 32];
-    int32_t red_s[CT_THREADS / 32];
     int red_ok[CT_THREADS / 32];
     double self_part[CT_THREADS / 32];
     double counter0;
@@ -756,14 +930,12 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
         const double counter0 = sh.counter0;
         selfLoop = sh.self_part[0];
         const double vd = a.vdeg[v];
-        double ccDeg;
-        int32_t ccSize;
-        load_comm(a, cc, ccDeg, ccSize);
+        const double ccDeg = __ldg(a.cdeg + cc);
         const double eix = __dsub_rn(counter0, selfLoop);
         const double ax = __dsub_rn(ccDeg, vd);
-        double gain = 0.0;
-        int32_t cand = INT_MAX, csz = 0;
-        bool ok = false;
+        double gain;
+        int32_t cand;
+        bool ok;
         // the other communities, compacted to the front of the table in slot order:
         // a kept slot moves to the count of kept slots before it, so no write lands
         // on a slot not yet read (each group's reads end at the barrier before its
@@ -792,51 +964,11 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
             nk += tot;
             __syncthreads();
         }
-        // four candidates per thread per round, their community loads issued together
-        for (int64_t i0 = 0; i0 < nk; i0 += 4 * CT_THREADS) {
-            int32_t kq[4], sq[4];
-            double aq[4], vq[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int64_t i = i0 + j * CT_THREADS + threadIdx.x;
-                kq[j] = i < nk ? keys[i] : EMPTY;
-                vq[j] = i < nk ? vals[i] : 0.0;
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                aq[j] = 0.0;
-                sq[j] = 0;
-                if (kq[j] != EMPTY) load_comm(a, kq[j], aq[j], sq[j]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                if (kq[j] == EMPTY) continue;
-                const double g = gain_of(vq[j], eix, vd, aq[j], ax, cst);
-                if (g > 0.0 && better(true, g, kq[j], ok, gain, cand, a.ref)) {
-                    gain = g;
-                    cand = kq[j];
-                    csz = sq[j];
-                    ok = true;
-                }
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double og = __shfl_xor_sync(full, gain, o);
-            const int32_t oc = __shfl_xor_sync(full, cand, o);
-            const int32_t os = __shfl_xor_sync(full, csz, o);
-            const bool ook = __shfl_xor_sync(full, (int)ok, o) != 0;
-            if (better(ook, og, oc, ok, gain, cand, a.ref)) {
-                gain = og;
-                cand = oc;
-                csz = os;
-                ok = true;
-            }
-        }
+        // each warp its own slots (warp * 32 + lane + k * CT_THREADS), then the warps' bests
+        warp_best(a, keys, vals, warp * 32, CT_THREADS, nk, eix, vd, ax, cst, ok, gain, cand);
         if (lane == 0) {
             sh.red_g[warp] = gain;
             sh.red_c[warp] = cand;
-            sh.red_s[warp] = csz;
             sh.red_ok[warp] = ok;
         }
         __syncthreads();
@@ -845,10 +977,11 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
                 if (better(sh.red_ok[w] != 0, sh.red_g[w], sh.red_c[w], ok, gain, cand, a.ref)) {
                     gain = sh.red_g[w];
                     cand = sh.red_c[w];
-                    csz = sh.red_s[w];
                     ok = true;
                 }
             }
+            int32_t ccSize, csz;
+            sizes_for_rule(a, ok, cand, cc, ccSize, csz);
             commit_vertex(a, v, cc, ccSize, vd, d > 0, counter0, ok, cand, csz);
         }
         __syncthreads();
@@ -1241,9 +1374,10 @@ __global__ void k_init(int64_t nv, const double *__restrict__ vdeg, double *__re
                        int32_t *__restrict__ past,
                        int32_t *__restrict__ curr, int32_t *__restrict__ target,
                        uint8_t *__restrict__ active, double *__restrict__ pcurr,
-                       double *__restrict__ pprev) {
+                       double *__restrict__ pprev, int32_t *__restrict__ noprune) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
          i += (int64_t)gridDim.x * blockDim.x) {
+        if (noprune && !(vdeg[i] >= 0.0)) *noprune = 1; // negative or NaN degree
         cdeg[i] = vdeg[i];
         csize[i] = 1;
         CommInfo z;
@@ -1334,7 +1468,8 @@ __global__ void __launch_bounds__(SEG_THREADS) k_apply_seg(
     const int64_t *__restrict__ voff, const int64_t *__restrict__ cb, int64_t J, int64_t C,
     double *__restrict__ cdeg, int32_t *__restrict__ csize, CommInfo *__restrict__ cupd,
     const double *__restrict__ cw, const uint8_t *__restrict__ active,
-    const uint8_t *__restrict__ jdone, int do_sums, double *__restrict__ part) {
+    const uint8_t *__restrict__ jdone, int do_sums, double *__restrict__ part,
+    int32_t *__restrict__ noprune) {
     __shared__ double ws[32];
     for (int64_t q = blockIdx.x; q < C; q += gridDim.x) {
         const int64_t j = seg_of_chunk(cb, J, q);
@@ -1348,7 +1483,11 @@ __global__ void __launch_bounds__(SEG_THREADS) k_apply_seg(
             if (u.size != 0 || u.deg != 0.0) {
                 cd = __dadd_rn(cdeg[i], u.deg);
                 cdeg[i] = cd;
-                csize[i] += u.size;
+                const int32_t ns = csize[i] + u.size;
+                csize[i] = ns;
+                // a community with members must keep a degree >= 0 for the pruning
+                // bound (rounding can leave an emptied one at -0.0 or a tiny negative)
+                if (noprune && ns > 0 && !(cd >= 0.0)) *noprune = 1;
                 CommInfo z;
                 z.deg = 0.0;
                 z.size = 0;
@@ -1956,6 +2095,8 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         }
     }
     const int grid = vg_grid(ctx, nv, 256);
+    DevBuf<int32_t> noprune(ctx, 1); // see can_prune
+    VG_CUDA(cudaMemsetAsync(noprune.p, 0, sizeof(int32_t), ctx->stream));
     if (nv) {
         vertex_degrees(ctx, g, vdeg.p, (int)vg_weights_integral(ctx, g));
     }
@@ -1964,7 +2105,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
     if (nv) {
         LaunchTimer lt(ctx);
         k_init<<<grid, 256, 0, ctx->stream>>>(nv, vdeg.p, cdeg.p, csize.p, cupd.p, A.p, B.p,
-                                              C.p, active.p, pA.p, pB.p);
+                                              C.p, active.p, pA.p, pB.p, noprune.p);
     }
     VG_CHECK_LAUNCH();
     Buckets bk;
@@ -2007,6 +2148,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         a.frozen = frozen.p;
         a.active = use_et ? active.p : nullptr;
         a.ref = g->ref;
+        a.noprune = noprune.p;
         a.ne = g->ne;
         a.constant = constant;
         if (timing) VG_CUDA(cudaEventRecord(ev0, ctx->stream));
@@ -2016,7 +2158,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
                 LaunchTimer lt(ctx);
                 k_apply_seg<<<agrid, SEG_THREADS, 0, ctx->stream>>>(
                     seg.voff.p, seg.cb.p, 1, seg.C, cdeg.p, csize.p, cupd.p, cw.p, a.active,
-                    nullptr, 0, part.p);
+                    nullptr, 0, part.p, noprune.p);
                 VG_CHECK_LAUNCH();
             }
         }
@@ -2026,7 +2168,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
                 LaunchTimer lt(ctx);
                 k_apply_seg<<<agrid, SEG_THREADS, 0, ctx->stream>>>(
                     seg.voff.p, seg.cb.p, 1, seg.C, cdeg.p, csize.p, cupd.p, cw.p, a.active,
-                    nullptr, 1, part.p);
+                    nullptr, 1, part.p, noprune.p);
             }
             VG_CHECK_LAUNCH();
             {
@@ -2129,6 +2271,8 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
     DevBuf<CommInfo> cupd(ctx, nv);
     DevBuf<int32_t> B0(ctx, nv), B1(ctx, nv), B2(ctx, nv);
     const int grid = vg_grid(ctx, nv, 256);
+    DevBuf<int32_t> noprune(ctx, 1); // see can_prune
+    VG_CUDA(cudaMemsetAsync(noprune.p, 0, sizeof(int32_t), ctx->stream));
     vertex_degrees(ctx, U, vdeg.p, (int)vg_weights_integral(ctx, U));
     // per-graph 2m in each graph's own fixed order, 1/(2m) on the host as in the plain path
     DevBuf<double> jconst(ctx, J);
@@ -2147,7 +2291,7 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
     {
         LaunchTimer lt(ctx);
         k_init<<<grid, 256, 0, ctx->stream>>>(nv, vdeg.p, cdeg.p, csize.p, cupd.p, B0.p, B1.p, B2.p,
-                                              nullptr, nullptr, nullptr);
+                                              nullptr, nullptr, nullptr, noprune.p);
     }
     VG_CHECK_LAUNCH();
     Buckets bk;
@@ -2187,6 +2331,7 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
         a.cupd = cupd.p;
         a.cw = cw.p;
         a.ref = U->ref;
+        a.noprune = noprune.p;
         a.ne = U->ne;
         a.constant = 0.0;
         a.vjob = vjob;
@@ -2200,7 +2345,8 @@ void vg_phase_batch_internal(vg_ctx *ctx, vg_graph *U, int64_t J, const int64_t 
             LaunchTimer lt(ctx);
             k_apply_seg<<<agrid, SEG_THREADS, 0, ctx->stream>>>(seg.voff.p, seg.cb.p, J, seg.C,
                                                                 cdeg.p, csize.p, cupd.p, cw.p,
-                                                                nullptr, done.p, 1, part.p);
+                                                                nullptr, done.p, 1, part.p,
+                                                                noprune.p);
         }
         VG_CHECK_LAUNCH();
         BatchDecide bd;

@@ -1,15 +1,20 @@
 """Served Louvain: a request loop over one running batch (continuous batching).
 
-Requests (a device graph and its run parameters) arrive over time. Whenever the
-device is free between rounds, every request that has arrived is submitted to the
-batch; the batch admits what fits its device-memory budget, runs one round (one
-phase for every graph in it, then the rebuild), and the graphs whose level loop
-ended are handed back with their latency (finish time - arrival time). Work of
-requests that arrive while others run overlaps on the device in the same
-launches, and each result is the one a run of its own gives.
+Requests arrive over time, each a graph in host memory (Vite's CSR: row offsets and
+Edge records, pinned memory copies fastest) or already on the device, with its run
+parameters. Whenever the device is free between rounds, the requests that have
+arrived are admitted in arrival order while their estimated device footprint fits
+the memory budget (a request larger than the whole budget runs alone); an admitted
+host request is uploaded then, so its copy is part of its latency. The batch runs
+one round (one phase for every graph in it, then the rebuild), and the graphs whose
+level loop ended are handed back with their latency (finish time - arrival time),
+releasing their share of the budget. Work of requests that arrive while others run
+overlaps on the device in the same launches, and each result is the one a run of its
+own gives.
 
-``sequential`` is the plain path the batch is measured against: one
-vg_louvain_run per request in arrival order, a single FIFO server.
+``sequential`` is the plain path the batch is measured against: per request in
+arrival order, the upload (for host requests) and one vg_louvain_run, a single FIFO
+server.
 """
 from __future__ import annotations
 
@@ -23,10 +28,31 @@ from . import Batch, Context, Graph
 
 @dataclass
 class Request:
-    graph: Graph
+    graph: Graph | None         # a device graph, or None for a host request
     arrival: float              # seconds after the start of the stream
     threshold: float = 1e-6
     want_comm: bool = False
+    rowptr: np.ndarray | None = None   # host request: int64 row offsets (nv + 1)
+    edges: np.ndarray | None = None    # host request: Vite Edge records (EDGE_DTYPE)
+
+    @property
+    def nv(self) -> int:
+        return self.graph.nv if self.graph is not None else len(self.rowptr) - 1
+
+    @property
+    def ne(self) -> int:
+        return self.graph.ne if self.graph is not None else len(self.edges)
+
+    def footprint(self) -> int:
+        """The batch's own estimate of a graph's device memory: 40 bytes per CSR entry,
+        200 per vertex and 1 MiB."""
+        return 40 * self.ne + 200 * self.nv + (1 << 20)
+
+    def device_graph(self, ctx: Context) -> tuple[Graph, bool]:
+        """(the graph on the device, whether it was uploaded here and so is owned)."""
+        if self.graph is not None:
+            return self.graph, False
+        return ctx.upload_edges(self.rowptr, self.edges), True
 
 
 @dataclass
@@ -57,6 +83,8 @@ def _lane_loop(ctx: Context, requests: list[Request], mine: list[int], budget: i
                clock, out: dict, info: dict) -> None:
     """One batch fed with the requests `mine` (sorted by arrival) in real time."""
     jobs: dict[int, int] = {}
+    held: dict[int, int] = {}  # job -> its footprint while admitted
+    inflight = 0
     rounds = 0
     with Batch(ctx, budget) as b:
         nxt = 0
@@ -64,10 +92,19 @@ def _lane_loop(ctx: Context, requests: list[Request], mine: list[int], budget: i
         done = 0
         while done < len(mine):
             now = clock() - t0
+            # admission: arrived requests in arrival order while their footprint fits
+            # the budget; with nothing admitted the next one runs whatever its size
             while nxt < len(mine) and requests[mine[nxt]].arrival <= now:
                 i = mine[nxt]
                 r = requests[i]
-                jobs[b.submit(r.graph, threshold=r.threshold, want_comm=r.want_comm)] = i
+                need = r.footprint()
+                if budget and inflight > 0 and inflight + need > budget:
+                    break
+                g, owned = r.device_graph(ctx)
+                j = b.submit(g, threshold=r.threshold, want_comm=r.want_comm, take=owned)
+                jobs[j] = i
+                held[j] = need
+                inflight += need
                 nxt += 1
                 busy = True
             if not busy:
@@ -81,6 +118,7 @@ def _lane_loop(ctx: Context, requests: list[Request], mine: list[int], budget: i
             t = clock() - t0
             for j in b.poll():
                 i = jobs.pop(j)
+                inflight -= held.pop(j)
                 res = b.result(j, want_comm=requests[i].want_comm)
                 out[i] = Served(i, requests[i].arrival, t, res.stats, res.comm)
                 b.forget(j)
@@ -103,7 +141,7 @@ def serve(ctx: Context, requests: list[Request], budget: int = 0, lanes=(),
     import threading
 
     bounds = sorted(lanes)
-    sizes = [r.graph.ne for r in requests]
+    sizes = [r.ne for r in requests]
     cls = [sum(1 for x in bounds if s > x) for s in sizes]
     nl = len(bounds) + 1
     order = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
@@ -120,8 +158,7 @@ def serve(ctx: Context, requests: list[Request], budget: int = 0, lanes=(),
                 share = sum(sizes[i] for i in mine[k]) / tot
                 # at least room for the lane's largest graph (the batch's own estimate:
                 # 40 bytes per CSR entry, 200 per vertex, 1 MiB)
-                big = max(40 * requests[i].graph.ne + 200 * requests[i].graph.nv + (1 << 20)
-                          for i in mine[k])
+                big = max(requests[i].footprint() for i in mine[k])
                 bud = 0 if budget == 0 else max(int(budget * share), big)
                 _lane_loop(ctxs[k], requests, mine[k], bud, t0, clock, out, infos[k])
         except BaseException as e:  # re-raised in the caller
@@ -159,7 +196,8 @@ def fifo(arrivals, service) -> np.ndarray:
 
 
 def sequential(ctx: Context, requests: list[Request], repeats: int = 1) -> ServeReport:
-    """The plain path: each request alone through vg_louvain_run, FIFO by arrival.
+    """The plain path: each request alone (its upload, for a host request, then
+    vg_louvain_run), FIFO by arrival.
 
     Service times are measured back to back (the whole sequence `repeats` times, each
     request's fastest time kept); the FIFO queue (start = max(arrival, previous
@@ -177,7 +215,10 @@ def sequential(ctx: Context, requests: list[Request], repeats: int = 1) -> Serve
             r = requests[i]
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            res = ctx.run(r.graph, threshold=r.threshold, want_comm=r.want_comm)
+            g, owned = r.device_graph(ctx)
+            res = ctx.run(g, threshold=r.threshold, want_comm=r.want_comm)
+            if owned:
+                g.free()
             e1.record(stream)
             e1.synchronize()
             t = e0.elapsed_time(e1) * 1e-3
