@@ -102,6 +102,11 @@ extern "C" vg_status vg_ctx_create(int device, size_t mem_budget_bytes, vg_ctx *
         ctx->budget = mem_budget_bytes;
         VG_CUDA(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
         VG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        // the side stream and its fork/join events exist from the start, so that a
+        // fork inside a stream capture creates nothing
+        VG_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+        VG_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+        VG_CUDA(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
         // keep freed blocks in the stream-ordered pool instead of returning them
         cudaMemPool_t pool;
         VG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
@@ -117,16 +122,31 @@ extern "C" vg_status vg_ctx_create(int device, size_t mem_budget_bytes, vg_ctx *
     return VG_OK;
 }
 
+cudaStream_t vg_side_fork(vg_ctx *ctx) {
+    VG_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
+    VG_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
+    return ctx->side;
+}
+
+void vg_side_join(vg_ctx *ctx) {
+    VG_CUDA(cudaEventRecord(ctx->join, ctx->side));
+    VG_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
+}
+
 extern "C" vg_status vg_ctx_destroy(vg_ctx *ctx) {
     if (!ctx) return VG_ERR_ARG;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->side) cudaStreamSynchronize(ctx->side);
     for (auto &pr : ctx->pending) ctx->event_pool.push_back(pr);
     for (auto &pr : ctx->event_pool) {
         cudaEventDestroy(pr.first);
         cudaEventDestroy(pr.second);
     }
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
+    if (ctx->join) cudaEventDestroy(ctx->join);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return VG_OK;

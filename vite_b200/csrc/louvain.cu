@@ -447,6 +447,9 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? VG_T16_MINB : VG_T32_MINB)) k_s
         const int32_t cc = __ldg(a.curr + v);
         const double vd = a.vdeg[v];
         const double ccDeg = __ldg(a.cdeg + cc);
+        // the 32-slot kernel's loops end at the largest degree among the lanes here (at
+        // least each lane's own): they take the same vertex class in position order
+        const int dmax = T > 16 ? (int)__reduce_max_sync(__activemask(), (unsigned)d) : T;
         int32_t c[T];
         uint32_t selfm = 0; // bit j: edge j is a self loop
         {
@@ -455,6 +458,7 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? VG_T16_MINB : VG_T32_MINB)) k_s
             int32_t t[T];
 #pragma unroll
             for (int j = 0; j < T; j++) {
+                if (j >= dmax) break;
                 t[j] = -1;
                 if (j < d) {
                     t[j] = __ldcs(a.tail + e0 + j);
@@ -463,6 +467,7 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? VG_T16_MINB : VG_T32_MINB)) k_s
             }
 #pragma unroll
             for (int j = 0; j < T; j++) {
+                if (j >= dmax) break;
                 c[j] = -1;
                 if (j < d) {
                     c[j] = __ldg(a.curr + t[j]);
@@ -472,34 +477,41 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? VG_T16_MINB : VG_T32_MINB)) k_s
         }
         cp_async_wait_all();
         double selfLoop = 0.0;
+        if (selfm) {
 #pragma unroll
-        for (int j = 0; j < T; j++)
-            if ((selfm >> j) & 1u) selfLoop = __dadd_rn(selfLoop, ssum[j][tid]);
+            for (int j = 0; j < T; j++) {
+                if (j >= dmax) break;
+                if ((selfm >> j) & 1u) selfLoop = __dadd_rn(selfLoop, ssum[j][tid]);
+            }
+        }
         // counters fold in place at the slot of each community's first occurrence,
         // in CSR order (slot j still holds w_j when edge j is folded: only first
         // occurrences receive additions)
         uint32_t first = 0; // bit j: edge j is the first occurrence of its community
+        int j0 = -1;        // first occurrence of the current community
 #pragma unroll
         for (int j = 0; j < T; j++) {
+            if (j >= dmax) break;
             if (j < d) {
                 int fj = j;
 #pragma unroll
                 for (int k = j - 1; k >= 0; k--)
                     if (c[k] == c[j]) fj = k;
-                if (fj == j) first |= 1u << j;
-                else ssum[fj][tid] = __dadd_rn(ssum[fj][tid], ssum[j][tid]);
+                if (fj == j) {
+                    first |= 1u << j;
+                    if (c[j] == cc) j0 = j;
+                } else {
+                    ssum[fj][tid] = __dadd_rn(ssum[fj][tid], ssum[j][tid]);
+                }
             }
         }
-        double counter0 = 0.0;
-#pragma unroll
-        for (int j = 0; j < T; j++)
-            if (((first >> j) & 1u) && c[j] == cc) counter0 = ssum[j][tid];
+        const double counter0 = j0 >= 0 ? ssum[j0][tid] : 0.0;
         const double eix = __dsub_rn(counter0, selfLoop);
         const double ax = __dsub_rn(ccDeg, vd);
         double bg;
         int32_t bc;
         bool ok;
-        best_of_row<T>(a, c, first, cc, &ssum[0][tid], NT, eix, vd, ax, cst, T, ok, bg, bc);
+        best_of_row<T>(a, c, first, cc, &ssum[0][tid], NT, eix, vd, ax, cst, dmax, ok, bg, bc);
         // the singleton rule (louvain.cpp:2275-2276) needs the sizes only when
         // the winner's id is larger than the current community's
         int32_t ccSize = 0, bs = 0;
@@ -1968,89 +1980,103 @@ static void plan_hubs(vg_ctx *ctx, const vg_graph *g, const Buckets &bk, int64_t
 }
 
 // one sweep over the hubs of color k
-static void sweep_hubs(vg_ctx *ctx, const SweepArgs &a, HubPlan &hp, int64_t k) {
+static void sweep_hubs(vg_ctx *ctx, const SweepArgs &a, HubPlan &hp, int64_t k,
+                       cudaStream_t st) {
     const int64_t q0 = hp.first[k], q1 = hp.first[k + 1];
     if (q1 == q0) return;
     const int64_t nch = hp.hcb[q1] - hp.hcb[q0], nsl = hp.hsb[q1] - hp.hsb[q0];
     const int64_t cap_blocks = 8LL * ctx->sm_count;
     {
         LaunchTimer lt(ctx);
-        k_hub_accum<<<(int)std::min(nch, cap_blocks), HUB_THREADS, 0, ctx->stream>>>(
+        k_hub_accum<<<(int)std::min(nch, cap_blocks), HUB_THREADS, 0, st>>>(
             a, hp.vtx.p, hp.toff.p, hp.cb.p, q0, q1, hp.keys.p, hp.vals.p, hp.self.p);
     }
     VG_CHECK_LAUNCH();
     {
         LaunchTimer lt(ctx);
-        k_hub_c0<<<vg_grid(ctx, q1 - q0, 256), 256, 0, ctx->stream>>>(
+        k_hub_c0<<<vg_grid(ctx, q1 - q0, 256), 256, 0, st>>>(
             a, hp.vtx.p, hp.toff.p, q0, q1, hp.keys.p, hp.vals.p, hp.c0.p);
     }
     VG_CHECK_LAUNCH();
     {
         LaunchTimer lt(ctx);
-        k_hub_eval<<<(int)std::min(nsl, cap_blocks), HUB_THREADS, 0, ctx->stream>>>(
+        k_hub_eval<<<(int)std::min(nsl, cap_blocks), HUB_THREADS, 0, st>>>(
             a, hp.vtx.p, hp.toff.p, hp.sb.p, q0, q1, hp.keys.p, hp.vals.p, hp.self.p, hp.c0.p,
             hp.best.p);
     }
     VG_CHECK_LAUNCH();
     {
         LaunchTimer lt(ctx);
-        k_hub_commit<<<vg_grid(ctx, (q1 - q0) * 32, 256), 256, 0, ctx->stream>>>(
+        k_hub_commit<<<vg_grid(ctx, (q1 - q0) * 32, 256), 256, 0, st>>>(
             a, hp.vtx.p, hp.sb.p, q0, q1, hp.self.p, hp.c0.p, hp.best.p);
     }
     VG_CHECK_LAUNCH();
 }
 
 // launch the sweep kernels over one color bucket; with `natural` the low-degree
-// class runs over all vertices in id order instead of its list
+// class runs over all vertices in id order instead of its list. The classes touch
+// disjoint vertices (reading the community arrays, which no sweep kernel writes, and
+// adding to the deltas with atomics), so when the first class and another one both
+// have work, the other classes run on the context's side stream alongside the first
+// (their blocks fill the SMs the first one's tail leaves idle); with profiling on,
+// every launch stays on the main stream so that each one is timed alone.
 static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64_t color,
                         HubPlan &hp, bool natural, int64_t nv) {
     const int32_t *list = b.list.p;
-    for (int cls = 0; cls < NCLS; cls++) {
-        const int64_t s = b.start[color * NCLS + cls], e = b.start[color * NCLS + cls + 1];
-        const int64_t n = e - s;
-        if (cls == 0 && natural) {
-            if (nv == 0) continue;
-            LaunchTimer lt(ctx);
-            const int64_t tiles_blocks = (nv + TILE_WARPS * 32 - 1) / (TILE_WARPS * 32);
-            const int tgrid = (int)std::max<int64_t>(
-                1, std::min<int64_t>(tiles_blocks,
-                                     (int64_t)effective_tuning(ctx).tile_grid * ctx->sm_count));
-            k_sweep_tile<TMAX><<<tgrid, TILE_WARPS * 32, 0, ctx->stream>>>(a, nv);
-            VG_CHECK_LAUNCH();
-            continue;
-        }
+    auto count = [&](int cls) { return b.start[color * NCLS + cls + 1] - b.start[color * NCLS + cls]; };
+    const bool first_busy = natural ? nv > 0 : count(0) > 0;
+    bool others = false;
+    for (int cls = 1; cls < NCLS; cls++) others = others || count(cls) > 0;
+    const bool fork = first_busy && others && !ctx->profile;
+    cudaStream_t st = fork ? vg_side_fork(ctx) : ctx->stream;
+    for (int cls = 1; cls < NCLS; cls++) {
+        const int64_t s = b.start[color * NCLS + cls];
+        const int64_t n = count(cls);
         if (n == 0) continue;
         if (cls == NCLS - 1) { // the hubs
-            sweep_hubs(ctx, a, hp, color);
+            sweep_hubs(ctx, a, hp, color, st);
             continue;
         }
         LaunchTimer lt(ctx);
         switch (cls) {
-        case 0:
-            k_sweep_thread<true, TMAX, TB><<<vg_grid(ctx, n, TB, 8), TB, 0, ctx->stream>>>(a, list + s, n);
-            break;
         case 1:
-            k_sweep_thread<true, 32, 128><<<vg_grid(ctx, n, 128, VG_T32_GRID), 128, 0, ctx->stream>>>(a, list + s, n);
+            k_sweep_thread<true, 32, 128><<<vg_grid(ctx, n, 128, VG_T32_GRID), 128, 0, st>>>(a, list + s, n);
             break;
         case 2:
             k_sweep_warp<WS_CAP, WS_WARPS><<<vg_grid(ctx, n * 32, WS_WARPS * 32, VG_WS_GRID), WS_WARPS * 32,
-                                             warp_smem_bytes<WS_CAP, WS_WARPS>(), ctx->stream>>>(
+                                             warp_smem_bytes<WS_CAP, WS_WARPS>(), st>>>(
                 a, list + s, n);
             break;
         case 3:
             k_sweep_warp<WT_CAP, WT_WARPS><<<vg_grid(ctx, n * 32, WT_WARPS * 32, VG_WS_GRID), WT_WARPS * 32,
-                                             warp_smem_bytes<WT_CAP, WT_WARPS>(), ctx->stream>>>(
+                                             warp_smem_bytes<WT_CAP, WT_WARPS>(), st>>>(
                 a, list + s, n);
             break;
         case 4:
             k_sweep_cta<<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, VG_CT_GRID), CT_THREADS, cta_smem_bytes(),
-                          ctx->stream>>>(a, list + s, n);
+                          st>>>(a, list + s, n);
             break;
         default:
             break;
         }
         VG_CHECK_LAUNCH();
     }
+    if (first_busy) {
+        LaunchTimer lt(ctx);
+        if (natural) {
+            const int64_t tiles_blocks = (nv + TILE_WARPS * 32 - 1) / (TILE_WARPS * 32);
+            const int tgrid = (int)std::max<int64_t>(
+                1, std::min<int64_t>(tiles_blocks,
+                                     (int64_t)effective_tuning(ctx).tile_grid * ctx->sm_count));
+            k_sweep_tile<TMAX><<<tgrid, TILE_WARPS * 32, 0, ctx->stream>>>(a, nv);
+        } else {
+            const int64_t n = count(0);
+            k_sweep_thread<true, TMAX, TB><<<vg_grid(ctx, n, TB, 8), TB, 0, ctx->stream>>>(
+                a, list + b.start[color * NCLS], n);
+        }
+        VG_CHECK_LAUNCH();
+    }
+    if (fork) vg_side_join(ctx);
 }
 
 struct PhaseTiming {

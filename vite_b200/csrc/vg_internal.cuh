@@ -59,7 +59,17 @@ struct vg_ctx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> event_pool;
     // sweep launch tuning (vg_ctx_set_tuning / vg_autotune); all zero = built-in defaults
     vg_tuning tune{};
+    // a second stream for kernels that may overlap the main stream's (vg_side_stream),
+    // with the events that fork it from and join it back to the main stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
+
+// the context's side stream: work enqueued on the stream vg_side_fork returns, up to
+// vg_side_join, runs concurrently with the main stream's (both ordered after what the
+// main stream held at the fork; the main stream's later work waits for the join)
+cudaStream_t vg_side_fork(vg_ctx *ctx);
+void vg_side_join(vg_ctx *ctx);
 
 // stream-ordered device allocation accounted against the context budget
 void *vg_alloc(vg_ctx *ctx, size_t bytes);
