@@ -174,8 +174,16 @@ __device__ void bitonic(uint64_t *sk, int n2, int t, int nt) {
 #ifndef VG_RH_GRID
 #define VG_RH_GRID 3 // CTAs per SM in the grid of k_rows_hash
 #endif
-constexpr int H_MAXU = 256;
-constexpr int H_CAP = 512;
+#ifndef VG_H_MAXU
+#define VG_H_MAXU 256 // most distinct keys of a segment on the table path
+#endif
+#ifndef VG_H_CAP
+#define VG_H_CAP 512 // table slots per warp
+#endif
+constexpr int H_MAXU = VG_H_MAXU;
+constexpr int H_CAP = VG_H_CAP;
+// a chunk can add 32 keys to H_MAXU before the check: a third of the slots stay empty
+static_assert(2 * H_CAP >= 3 * (H_MAXU + 32), "the warp table must keep a third of its slots empty");
 constexpr int H_WARPS = 8;
 constexpr int32_t H_EMPTY = -1;
 

@@ -131,8 +131,9 @@ __global__ void k_gather_deg(const int64_t *__restrict__ rowptr, const int32_t *
 }
 
 // new row k = old row from[k] (starting at src_start[k]), tails renamed through
-// `rename`, entry order kept; eight lanes per row (rows are short), two entries per
-// lane per step: both tails are loaded before the renames are gathered
+// `rename`, entry order kept; eight lanes per row (rows are short), two rows per
+// group of lanes at a time and two entries of each per lane per step: the four
+// tails and weights are loaded before the renames are gathered
 __global__ void k_move_rows(const int32_t *__restrict__ tail, const double *__restrict__ w, int64_t n,
                             const int64_t *__restrict__ src_start,
                             const int32_t *__restrict__ rename, const int64_t *__restrict__ rp2,
@@ -140,22 +141,33 @@ __global__ void k_move_rows(const int32_t *__restrict__ tail, const double *__re
     const int sub = threadIdx.x & 7;
     const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
     const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
-    for (int64_t k = grp; k < n; k += ng) {
-        const int64_t s = src_start[k], o = rp2[k], len = rp2[k + 1] - o;
-        for (int64_t j = sub; j < len; j += 16) {
-            const bool two = j + 8 < len;
-            const int32_t t0 = tail[s + j];
-            const int32_t t1 = two ? tail[s + j + 8] : 0;
-            const double w0 = w[s + j];
-            const double w1 = two ? w[s + j + 8] : 0.0;
-            const int32_t r0 = rename[t0];
-            const int32_t r1 = two ? rename[t1] : 0;
-            tail2[o + j] = r0;
-            w2[o + j] = w0;
-            if (two) {
-                tail2[o + j + 8] = r1;
-                w2[o + j + 8] = w1;
-            }
+    for (int64_t k = grp; k < n; k += 2 * ng) {
+        const int64_t kb = k + ng;
+        const bool hb = kb < n;
+        const int64_t sa = src_start[k], oa = rp2[k], la = rp2[k + 1] - oa;
+        const int64_t sb = hb ? src_start[kb] : 0, ob = hb ? rp2[kb] : 0;
+        const int64_t lb = hb ? rp2[kb + 1] - ob : 0;
+        const int64_t m = la > lb ? la : lb;
+        for (int64_t j = sub; j < m; j += 16) {
+            int32_t t[4] = {0, 0, 0, 0}, r[4];
+            double x[4] = {0.0, 0.0, 0.0, 0.0};
+            const bool h[4] = {j < la, j + 8 < la, j < lb, j + 8 < lb};
+            const int64_t src[4] = {sa + j, sa + j + 8, sb + j, sb + j + 8};
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (h[q]) {
+                    t[q] = tail[src[q]];
+                    x[q] = w[src[q]];
+                }
+#pragma unroll
+            for (int q = 0; q < 4; q++) r[q] = h[q] ? rename[t[q]] : 0;
+            const int64_t dst[4] = {oa + j, oa + j + 8, ob + j, ob + j + 8};
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (h[q]) {
+                    tail2[dst[q]] = r[q];
+                    w2[dst[q]] = x[q];
+                }
         }
     }
 }
@@ -286,20 +298,29 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
     if (!nv) return;
     DevBuf<int32_t> label(ctx, nv);
     DevBuf<uint8_t> dist(ctx, nv);
-    DevBuf<unsigned long long> claimed(ctx, 1);
-    unsigned long long *h = (unsigned long long *)vg_pinned(ctx, sizeof(unsigned long long));
+    // steps run in groups of BFS_GROUP, each with its own claim counter, and the
+    // counters are read back once per group: the search has ended at the first
+    // step that claimed nothing (the steps after it claim nothing either)
+    constexpr int BFS_GROUP = 4;
+    DevBuf<unsigned long long> claimed(ctx, BFS_GROUP);
+    unsigned long long *h =
+        (unsigned long long *)vg_pinned(ctx, BFS_GROUP * sizeof(unsigned long long));
     const int grid = vg_grid(ctx, nv, 256);
     { LaunchTimer lt(ctx); k_bfs_init<<<grid, 256, 0, ctx->stream>>>(nv, 0x5eedULL, label.p, dist.p); }
     VG_CHECK_LAUNCH();
-    for (int step = 1; step <= MAX_BFS_STEPS - 1; step++) {
-        VG_CUDA(cudaMemsetAsync(claimed.p, 0, sizeof(unsigned long long), ctx->stream));
-        { LaunchTimer lt(ctx);
-          k_bfs_step<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->tail, nv, step, label.p, dist.p,
-                                                    claimed.p); }
-        VG_CHECK_LAUNCH();
-        VG_CUDA(cudaMemcpyAsync(h, claimed.p, sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
+    bool done = false;
+    for (int step0 = 1; step0 <= MAX_BFS_STEPS - 1 && !done; step0 += BFS_GROUP) {
+        const int ns = std::min(BFS_GROUP, MAX_BFS_STEPS - step0);
+        VG_CUDA(cudaMemsetAsync(claimed.p, 0, BFS_GROUP * sizeof(unsigned long long), ctx->stream));
+        for (int k = 0; k < ns; k++) {
+            LaunchTimer lt(ctx);
+            k_bfs_step<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->tail, nv, step0 + k, label.p,
+                                                      dist.p, claimed.p + k);
+            VG_CHECK_LAUNCH();
+        }
+        VG_CUDA(cudaMemcpyAsync(h, claimed.p, ns * sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
         vg_sync(ctx);
-        if (*h == 0) break;
+        for (int k = 0; k < ns; k++) done = done || h[k] == 0;
     }
     DevBuf<uint64_t> keys(ctx, nv);
     DevBuf<uint32_t> vals(ctx, nv);
