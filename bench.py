@@ -57,7 +57,9 @@ SERVE_E = (1e3, 5e7)              # CSR entries, log-uniform
 SERVE_SEED = 5151
 SERVE_LOAD = 8.0                  # offered load in units of the plain path's capacity
 SERVE_BUDGET = 48 << 30           # device-memory budget of the serving batches
-SERVE_LANES = (1 << 16, 1 << 20, 1 << 23, 25_000_000)  # CSR-entry bounds of the size-class lanes
+SERVE_LANES = (1 << 16, 1 << 20, 1 << 23)  # CSR-entry bounds of the batched size-class lanes
+SERVE_DIRECT = 25_000_000         # larger requests run alone, two at a time (upload overlaps a run)
+SERVE_DIRECT_WORKERS = 2
 REL_TOL = 1e-9
 
 
@@ -498,7 +500,8 @@ def run_serving(ctx, count: int, lanes=SERVE_LANES) -> dict:
     fin = sv.fifo(arrivals, service)
     plain_lat = fin - arrivals
     ctx.reserve(SERVE_BUDGET)
-    served = sv.serve(ctx, reqs, budget=SERVE_BUDGET, lanes=lanes)
+    served = sv.serve(ctx, reqs, budget=SERVE_BUDGET, lanes=lanes, direct_above=SERVE_DIRECT,
+                      direct_workers=SERVE_DIRECT_WORKERS)
     lat = served.latencies()
     agree = sum(levels_agree(s.levels, p.levels) for s, p in zip(served.results, plain.results))
     gps = count / served.seconds
@@ -510,12 +513,14 @@ def run_serving(ctx, count: int, lanes=SERVE_LANES) -> dict:
                     f"RGG (distance weights) or Barabasi-Albert m=8 (U(0,1) weights), held in "
                     f"pinned host memory in Vite's layout and uploaded on admission; Poisson "
                     f"arrivals at {SERVE_LOAD:g}x the plain path's capacity, seed {SERVE_SEED}; "
-                    f"budget {SERVE_BUDGET >> 30} GiB, size-class lanes at "
-                    f"{'/'.join(str(x) for x in lanes)} CSR entries; full multi-level Louvain",
+                    f"budget {SERVE_BUDGET >> 30} GiB, batched size-class lanes at "
+                    f"{'/'.join(str(x) for x in lanes)} CSR entries, requests above "
+                    f"{SERVE_DIRECT} entries run alone on {SERVE_DIRECT_WORKERS} streams; full "
+                    f"multi-level Louvain",
         "requests": count, "csr_entries": int(sum(ne)), "rate_per_s": rate,
         "graphs_per_s": gps, "p50_s": sv.percentile(lat, 50),
         "p99_s": sv.percentile(lat, 99), "rounds": served.rounds,
-        "lanes": served.stats["lanes"],
+        "lanes": served.stats["lanes"], "direct": served.stats["direct"],
         "plain_graphs_per_s": plain_gps,
         "speedup_vs_plain": gps / plain_gps,
         "plain_p50_s": sv.percentile(plain_lat, 50), "plain_p99_s": sv.percentile(plain_lat, 99),

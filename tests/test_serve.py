@@ -72,3 +72,22 @@ def test_host_requests_uploaded_on_admission(ctx):
     for r, a in zip(seq.results, alone):
         assert [x["modularity"] for x in r.levels] == [x["modularity"] for x in a.stats]
     assert ctx.bytes_in_use == start  # every uploaded graph was released
+
+
+def test_direct_lane_results_equal_alone(ctx):
+    """Requests above `direct_above` entries run alone on the direct workers, the rest in
+    batched lanes; every result is still the one the graph gets alone."""
+    gs = [ctx.generate_rgg(1500 + 2500 * k, 0.0, 0) for k in range(6)]
+    for g in gs:
+        ctx.reweight(g, 1)
+    alone = [ctx.run(g, want_comm=True) for g in gs]
+    reqs = [sv.Request(g, arrival=0.001 * k, want_comm=True) for k, g in enumerate(gs)]
+    cut = sorted(g.ne for g in gs)[2]
+    rep = sv.serve(ctx, reqs, budget=1 << 30, lanes=(20000,), direct_above=cut, direct_workers=2)
+    assert rep.stats["direct"]["requests"] == sum(g.ne > cut for g in gs)
+    for r, a in zip(rep.results, alone):
+        assert [(x["nv"], x["ne"], x["iters"], x["modularity"]) for x in r.levels] == \
+               [(x["nv"], x["ne"], x["iters"], x["modularity"]) for x in a.stats]
+        assert np.array_equal(r.comm, a.comm)
+    for g in gs:
+        g.free()

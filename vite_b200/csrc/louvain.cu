@@ -1489,29 +1489,51 @@ __global__ void __launch_bounds__(SEG_THREADS) k_apply_seg(
         const int64_t lo = voff[j] + (q - cb[j]) * SEG_CHUNK;
         const int64_t hi = min(lo + SEG_CHUNK, voff[j + 1]);
         double le = 0.0, la2 = 0.0, frozen = 0.0;
-        for (int64_t i = lo + threadIdx.x; i < hi; i += SEG_THREADS) {
-            const CommInfo u = cupd[i];
-            double cd;
-            if (u.size != 0 || u.deg != 0.0) {
-                cd = __dadd_rn(cdeg[i], u.deg);
-                cdeg[i] = cd;
-                const int32_t ns = csize[i] + u.size;
-                csize[i] = ns;
-                // a community with members must keep a degree >= 0 for the pruning
-                // bound (rounding can leave an emptied one at -0.0 or a tiny negative)
-                if (noprune && ns > 0 && !(cd >= 0.0)) *noprune = 1;
-                CommInfo z;
-                z.deg = 0.0;
-                z.size = 0;
-                z.pad = 0;
-                cupd[i] = z;
-            } else {
-                cd = do_sums ? cdeg[i] : 0.0;
+        // a thread's entries i, i + SEG_THREADS, ... in that order (the sums' fixed
+        // order), four of them loaded together
+        constexpr int U4 = 4;
+        for (int64_t i0 = lo + threadIdx.x; i0 < hi; i0 += U4 * SEG_THREADS) {
+            CommInfo u[U4];
+            double cd0[U4], cwv[U4];
+#pragma unroll
+            for (int k = 0; k < U4; k++) {
+                const int64_t i = i0 + (int64_t)k * SEG_THREADS;
+                u[k].deg = 0.0;
+                u[k].size = 0;
+                cd0[k] = 0.0;
+                cwv[k] = 0.0;
+                if (i < hi) {
+                    u[k] = cupd[i];
+                    if (do_sums) {
+                        cd0[k] = cdeg[i];
+                        cwv[k] = cw[i];
+                    }
+                }
             }
-            if (do_sums) {
-                le = __dadd_rn(le, cw[i]);
-                la2 = __dadd_rn(la2, __dmul_rn(cd, cd));
-                if (active && !active[i]) frozen += 1.0;
+#pragma unroll
+            for (int k = 0; k < U4; k++) {
+                const int64_t i = i0 + (int64_t)k * SEG_THREADS;
+                if (i >= hi) break;
+                double cd = cd0[k];
+                if (u[k].size != 0 || u[k].deg != 0.0) {
+                    cd = __dadd_rn(do_sums ? cd : cdeg[i], u[k].deg);
+                    cdeg[i] = cd;
+                    const int32_t ns = csize[i] + u[k].size;
+                    csize[i] = ns;
+                    // a community with members must keep a degree >= 0 for the pruning
+                    // bound (rounding can leave an emptied one at -0.0 or a tiny negative)
+                    if (noprune && ns > 0 && !(cd >= 0.0)) *noprune = 1;
+                    CommInfo z;
+                    z.deg = 0.0;
+                    z.size = 0;
+                    z.pad = 0;
+                    cupd[i] = z;
+                }
+                if (do_sums) {
+                    le = __dadd_rn(le, cwv[k]);
+                    la2 = __dadd_rn(la2, __dmul_rn(cd, cd));
+                    if (active && !active[i]) frozen += 1.0;
+                }
             }
         }
         if (!do_sums) continue;

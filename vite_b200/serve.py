@@ -128,8 +128,32 @@ def _lane_loop(ctx: Context, requests: list[Request], mine: list[int], budget: i
         info["stats"] = b.stats()
 
 
+def _direct_loop(ctx: Context, requests: list[Request], queue: list[int], lock, t0: float,
+                 clock, out: dict, info: dict) -> None:
+    """One worker of the direct lane: takes the earliest arrived request left in the
+    shared queue, uploads it (host requests) and runs it alone (vg_louvain_run)."""
+    n = 0
+    while True:
+        with lock:
+            if not queue:
+                break
+            i = queue.pop(0)
+        r = requests[i]
+        wait = r.arrival - (clock() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        g, owned = r.device_graph(ctx)
+        res = ctx.run(g, threshold=r.threshold, want_comm=r.want_comm)
+        if owned:
+            g.free()
+        out[i] = Served(i, r.arrival, clock() - t0, res.stats, res.comm)
+        n += 1
+    info["rounds"] = n
+
+
 def serve(ctx: Context, requests: list[Request], budget: int = 0, lanes=(),
-          clock=time.perf_counter) -> ServeReport:
+          clock=time.perf_counter, direct_above: int | None = None,
+          direct_workers: int = 2) -> ServeReport:
     """Run the request stream in real time.
 
     lanes: ascending CSR-entry bounds; with k bounds the requests are split into k+1
@@ -137,24 +161,37 @@ def serve(ctx: Context, requests: list[Request], budget: int = 0, lanes=(),
     (the last class keeps `ctx`), so the rounds of small graphs are not held to
     the length of the largest graphs' phases. Each lane gets the whole budget
     divided in proportion to its share of the requests' entries.
+
+    direct_above: requests with more CSR entries than this skip batching (a graph
+    that size fills the GPU alone, and a batch would repack it whenever its lane's
+    membership changes): `direct_workers` host threads, each with its own context and
+    stream, take them in arrival order and run each alone, so one request's upload
+    overlaps another's run. Their memory is outside `budget` (one graph per worker).
     """
     import threading
 
     bounds = sorted(lanes)
     sizes = [r.ne for r in requests]
+    direct = [direct_above is not None and s > direct_above for s in sizes]
     cls = [sum(1 for x in bounds if s > x) for s in sizes]
     nl = len(bounds) + 1
     order = sorted(range(len(requests)), key=lambda i: requests[i].arrival)
-    mine = [[i for i in order if cls[i] == k] for k in range(nl)]
-    tot = max(sum(sizes), 1)
+    mine = [[i for i in order if cls[i] == k and not direct[i]] for k in range(nl)]
+    dqueue = [i for i in order if direct[i]]
+    nd = direct_workers if dqueue else 0
+    tot = max(sum(s for s, d in zip(sizes, direct) if not d), 1)
     ctxs = [ctx if k == nl - 1 else Context(ctx.device) for k in range(nl)]
+    dctxs = [Context(ctx.device) for _ in range(nd)]
     out: dict[int, Served] = {}
-    infos = [dict() for _ in range(nl)]
+    infos = [dict() for _ in range(nl + nd)]
     errors = []
+    lock = threading.Lock()
 
     def run(k, t0):
         try:
-            if mine[k]:
+            if k >= nl:
+                _direct_loop(dctxs[k - nl], requests, dqueue, lock, t0, clock, out, infos[k])
+            elif mine[k]:
                 share = sum(sizes[i] for i in mine[k]) / tot
                 # at least room for the lane's largest graph (the batch's own estimate:
                 # 40 bytes per CSR entry, 200 per vertex, 1 MiB)
@@ -166,7 +203,7 @@ def serve(ctx: Context, requests: list[Request], budget: int = 0, lanes=(),
 
     try:
         t0 = clock()
-        threads = [threading.Thread(target=run, args=(k, t0)) for k in range(nl)]
+        threads = [threading.Thread(target=run, args=(k, t0)) for k in range(nl + nd)]
         for t in threads:
             t.start()
         for t in threads:
@@ -174,14 +211,18 @@ def serve(ctx: Context, requests: list[Request], budget: int = 0, lanes=(),
     finally:
         for k in range(nl - 1):
             ctxs[k].close()
+        for c in dctxs:
+            c.close()
     if errors:
         raise errors[0]
     results = [out[i] for i in range(len(requests))]
     first = min(r.arrival for r in requests)
     last = max(r.finish for r in results)
     stats = {"lanes": [{"requests": len(mine[k]), "rounds": infos[k].get("rounds", 0)}
-                       for k in range(nl)]}
-    return ServeReport(results, last - first, sum(i.get("rounds", 0) for i in infos), stats)
+                       for k in range(nl)],
+             "direct": {"requests": sum(direct), "workers": nd,
+                        "above_entries": direct_above}}
+    return ServeReport(results, last - first, sum(i.get("rounds", 0) for i in infos[:nl]), stats)
 
 
 def fifo(arrivals, service) -> np.ndarray:
