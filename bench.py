@@ -40,7 +40,7 @@ N_VERTICES = 1 << 24
 EXTRA_PERCENT = 1.0
 SEED = 2024
 THRESHOLD = 1e-6
-REF_BUDGET_S = 1400.0      # reference arm: its timed runs end within this many seconds of its start
+REF_BUDGET_S = 1500.0      # reference arm: its timed runs end within this many seconds of its start
 METRIC = "Louvain e2e sec (RGG 2^24 +1% extra edges, full multi-level)"
 UNIT = "s"
 

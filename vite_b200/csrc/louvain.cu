@@ -106,6 +106,10 @@ struct SweepArgs {
     // negative or NaN (then candidate pruning is off); null: pruning off
     const int32_t *__restrict__ noprune;
     int64_t ne;                          // CSR entries (bounds of the vector loads)
+    // 1 when every vertex is still in its own community (curr[u] == u: a phase's first
+    // iteration, launched directly): the tile kernel then runs its instantiation
+    // without community gathers
+    int32_t ident;
     double constant;
     // batched graphs (null for one graph): the graph of each vertex, each graph's
     // 1/(2m), and the graphs whose phase has ended (their vertices are skipped)
@@ -525,7 +529,7 @@ __global__ void __launch_bounds__(NT, (T <= 16 ? VG_T16_MINB : VG_T32_MINB)) k_s
 
 // one vertex of a tile (degree d <= T): counters fold in place in the staged
 // weights of its row, in CSR order, at the slot of each community's first occurrence
-template <int T>
+template <int T, bool IDENT>
 __device__ __forceinline__ void tile_vertex(const SweepArgs &a, int32_t v, int d, int dmax,
                                             double cst, const int32_t *ts, double *ws, int32_t cc,
                                             double vd, double ccDeg) {
@@ -542,7 +546,7 @@ __device__ __forceinline__ void tile_vertex(const SweepArgs &a, int32_t v, int d
         c[j] = -1;
         if (j < d) {
             const int32_t t = ts[j];
-            c[j] = __ldg(a.curr + t);
+            c[j] = IDENT ? t : __ldg(a.curr + t);
             if (t == v) selfm |= 1u << j;
         }
     }
@@ -607,7 +611,7 @@ constexpr int TILE_CAP = 504;          // staged edges per warp (48 KB of shared
 #endif
 constexpr int TILE_WARPS = VG_TILE_WARPS;
 
-template <int T>
+template <int T, bool IDENT>
 __global__ void __launch_bounds__(TILE_WARPS * 32, VG_TILE_MINB) k_sweep_tile(SweepArgs a, int64_t nv) {
     static_assert(32 * T <= TILE_CAP + 8, "the per-lane fallback layout must fit the buffer");
     __shared__ __align__(16) int32_t st_all[TILE_WARPS][TILE_CAP + 8];
@@ -673,14 +677,15 @@ __global__ void __launch_bounds__(TILE_WARPS * 32, VG_TILE_MINB) k_sweep_tile(Sw
         int32_t cc = 0;
         double vd = 0.0, ccDeg = 0.0;
         if (live && d <= T) {
-            cc = __ldg(a.curr + v);
+            cc = IDENT ? v : __ldg(a.curr + v);
             vd = a.vdeg[v];
             ccDeg = __ldg(a.cdeg + cc);
         }
         const int dmax = (int)__reduce_max_sync(0xffffffffu, (live && d <= T) ? (unsigned)d : 0u);
         cp_async_wait_all();
         __syncwarp();
-        if (live && d <= T) tile_vertex<T>(a, v, d, dmax, cst, st + off_t, sw + off_w, cc, vd, ccDeg);
+        if (live && d <= T)
+            tile_vertex<T, IDENT>(a, v, d, dmax, cst, st + off_t, sw + off_w, cc, vd, ccDeg);
         __syncwarp();
     }
 }
@@ -2090,7 +2095,10 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
             const int tgrid = (int)std::max<int64_t>(
                 1, std::min<int64_t>(tiles_blocks,
                                      (int64_t)effective_tuning(ctx).tile_grid * ctx->sm_count));
-            k_sweep_tile<TMAX><<<tgrid, TILE_WARPS * 32, 0, ctx->stream>>>(a, nv);
+            if (a.ident)
+                k_sweep_tile<TMAX, true><<<tgrid, TILE_WARPS * 32, 0, ctx->stream>>>(a, nv);
+            else
+                k_sweep_tile<TMAX, false><<<tgrid, TILE_WARPS * 32, 0, ctx->stream>>>(a, nv);
         } else {
             const int64_t n = count(0);
             k_sweep_thread<true, TMAX, TB><<<vg_grid(ctx, n, TB, 8), TB, 0, ctx->stream>>>(
@@ -2198,6 +2206,7 @@ static void run_phase(vg_ctx *ctx, vg_graph *g, const vg_phase_params *p, double
         a.ref = g->ref;
         a.noprune = noprune.p;
         a.ne = g->ne;
+        a.ident = numIters == 1 ? 1 : 0; // k_init put every vertex in its own community
         a.constant = constant;
         if (timing) VG_CUDA(cudaEventRecord(ev0, ctx->stream));
         for (int64_t ci = 0; ci < numColor; ci++) {
