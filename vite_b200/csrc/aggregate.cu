@@ -169,43 +169,47 @@ __device__ void bitonic(uint64_t *sk, int n2, int t, int nt) {
 // peers' weights in lane order onto the key's running sum in a shared-memory
 // table, so every sum is the left fold in segment order. Only the distinct keys
 // are then sorted: in registers across the warp when there are at most 32 of
-// them, else in shared memory. A segment with more than H_MAXU distinct keys is
-// flagged for the sorted path.
+// them, else in shared memory. The reduction runs in two tiers: first every segment
+// with a small table (MAXU_S distinct keys at most, so more warps fit per SM), then
+// the segments that overflowed it with a large one (MAXU_L); a segment with more
+// than MAXU_L distinct keys is flagged for the sorted path.
 #ifndef VG_RH_GRID
-#define VG_RH_GRID 3 // CTAs per SM in the grid of k_rows_hash
+#define VG_RH_GRID 3 // CTAs per SM in the grid of the large-table tier
 #endif
-#ifndef VG_H_MAXU
-#define VG_H_MAXU 256 // most distinct keys of a segment on the table path
+#ifndef VG_RH_GRID_S
+#define VG_RH_GRID_S 5 // CTAs per SM in the grid of the small-table tier
 #endif
-#ifndef VG_H_CAP
-#define VG_H_CAP 512 // table slots per warp
-#endif
-constexpr int H_MAXU = VG_H_MAXU;
-constexpr int H_CAP = VG_H_CAP;
-// a chunk can add 32 keys to H_MAXU before the check: a third of the slots stay empty
-static_assert(2 * H_CAP >= 3 * (H_MAXU + 32), "the warp table must keep a third of its slots empty");
+constexpr int H_MAXU_S = 96, H_CAP_S = 256;  // small tier
+constexpr int H_MAXU = 256, H_CAP = 512;     // large tier
+// a chunk can add 32 keys to MAXU before the check: a third of the slots stay empty
+static_assert(2 * H_CAP >= 3 * (H_MAXU + 32) && 2 * H_CAP_S >= 3 * (H_MAXU_S + 32),
+              "a warp table must keep a third of its slots empty");
 constexpr int H_WARPS = 8;
 constexpr int32_t H_EMPTY = -1;
 
-struct HashWarpSmem {
-    int32_t keys[H_CAP];
-    double vals[H_CAP];
-    uint64_t list[H_MAXU + 32]; // (key << 32 | slot) of the distinct keys
+template <int CAP, int MAXU> struct HashWarpSmem {
+    int32_t keys[CAP];
+    double vals[CAP];
+    uint64_t list[MAXU + 32]; // (key << 32 | slot) of the distinct keys
     alignas(16) double stage[32];
 };
 
-
+// rows: null for every segment 0..nc-1, else the segments rows[0 .. *nrows)
+template <int CAP, int MAXU>
 __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
-    int64_t nc, const int64_t *__restrict__ rstart, const int32_t *__restrict__ gk,
+    int64_t nc, const int32_t *__restrict__ rows, const int64_t *__restrict__ nrows,
+    const int64_t *__restrict__ rstart, const int32_t *__restrict__ gk,
     const double *__restrict__ gw, int32_t *__restrict__ uk, double *__restrict__ uw,
     int64_t *__restrict__ ucount, int32_t *__restrict__ flag) {
     extern __shared__ unsigned char hsm_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    HashWarpSmem &S = reinterpret_cast<HashWarpSmem *>(hsm_raw)[warp];
+    HashWarpSmem<CAP, MAXU> &S = reinterpret_cast<HashWarpSmem<CAP, MAXU> *>(hsm_raw)[warp];
     const unsigned full = 0xffffffffu, lt = (1u << lane) - 1u;
     const int64_t wg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t row = wg; row < nc; row += nw) {
+    const int64_t n = rows ? *nrows : nc;
+    for (int64_t idx = wg; idx < n; idx += nw) {
+        const int64_t row = rows ? rows[idx] : idx;
         const int64_t b = rstart[row];
         const int64_t L = rstart[row + 1] - b;
         if (L <= 32) {
@@ -250,8 +254,8 @@ __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
             continue;
         }
         int logcap = 5;
-        while ((1 << logcap) < 2 * L && (1 << logcap) < H_CAP) logcap++;
-        const int cap = 1 << logcap; // > twice the distinct keys held (at most H_MAXU + 31)
+        while ((1 << logcap) < 2 * L && (1 << logcap) < CAP) logcap++;
+        const int cap = 1 << logcap; // > twice the distinct keys held (at most MAXU + 31)
         for (int s = lane; s < cap; s += 32) S.keys[s] = H_EMPTY;
         __syncwarp();
         int U = 0;
@@ -306,7 +310,7 @@ __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
                 if (fresh) S.list[U + __popc(fm & lt)] = ((uint64_t)(uint32_t)k << 32) | (uint32_t)slot;
                 U += __popc(fm);
                 __syncwarp();
-                if (U > H_MAXU) { // too many distinct keys for the table: the sorted path
+                if (U > MAXU) { // too many distinct keys for the table: the next tier
                     over = true;
                     break;
                 }
@@ -363,6 +367,14 @@ __global__ void __launch_bounds__(H_WARPS * 32) k_rows_hash(
         }
         __syncwarp();
     }
+}
+
+// the segments a tier flagged, listed in order (pos: exclusive scan of the flags)
+__global__ void k_list_flagged(int64_t nc, const int32_t *__restrict__ flag,
+                               const int64_t *__restrict__ pos, int32_t *__restrict__ rows) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nc;
+         r += (int64_t)gridDim.x * blockDim.x)
+        if (flag[r]) rows[pos[r]] = (int32_t)r;
 }
 
 // Segments with more than H_MAXU distinct keys, all together: every entry becomes the key
@@ -603,10 +615,16 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
                             const int32_t *key_to_pos) {
     const int64_t nv = g->nv, ne = g->ne;
     const int integral = g->integral == 1 ? 1 : 0; // every weight a small integer
+    using SmemS = HashWarpSmem<H_CAP_S, H_MAXU_S>;
+    using SmemL = HashWarpSmem<H_CAP, H_MAXU>;
     static bool configured = false;
     if (!configured) {
-        VG_CUDA(cudaFuncSetAttribute(k_rows_hash, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(H_WARPS * sizeof(HashWarpSmem))));
+        VG_CUDA(cudaFuncSetAttribute(k_rows_hash<H_CAP_S, H_MAXU_S>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(H_WARPS * sizeof(SmemS))));
+        VG_CUDA(cudaFuncSetAttribute(k_rows_hash<H_CAP, H_MAXU>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(H_WARPS * sizeof(SmemL))));
         configured = true;
     }
     int kbits = 1;
@@ -669,10 +687,28 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     DevBuf<int32_t> flag(ctx, nc);
     if (nc) {
         { LaunchTimer lt(ctx);
-          k_rows_hash<<<vg_grid(ctx, nc * 32, H_WARPS * 32, VG_RH_GRID), H_WARPS * 32,
-                        H_WARPS * sizeof(HashWarpSmem), ctx->stream>>>(
-              nc, rstart.p, gk.p, gw.p, uk.p, uw.p, ucount.p, flag.p); }
+          k_rows_hash<H_CAP_S, H_MAXU_S>
+              <<<vg_grid(ctx, nc * 32, H_WARPS * 32, VG_RH_GRID_S), H_WARPS * 32,
+                 H_WARPS * sizeof(SmemS), ctx->stream>>>(nc, nullptr, nullptr, rstart.p, gk.p, gw.p,
+                                                         uk.p, uw.p, ucount.p, flag.p); }
         VG_CHECK_LAUNCH();
+        {
+            // the segments that overflowed the small table, with the large one (their
+            // count stays on the device; the grid covers every segment's warp)
+            DevBuf<int64_t> fpos(ctx, nc), fcount(ctx, 1);
+            DevBuf<int32_t> frows(ctx, nc);
+            vg_scan_i32_async(ctx, flag.p, fpos.p, nc, fcount.p);
+            { LaunchTimer lt(ctx);
+              k_list_flagged<<<vg_grid(ctx, nc, 256), 256, 0, ctx->stream>>>(nc, flag.p, fpos.p,
+                                                                              frows.p); }
+            VG_CHECK_LAUNCH();
+            { LaunchTimer lt(ctx);
+              k_rows_hash<H_CAP, H_MAXU>
+                  <<<vg_grid(ctx, nc * 32, H_WARPS * 32, VG_RH_GRID), H_WARPS * 32,
+                     H_WARPS * sizeof(SmemL), ctx->stream>>>(nc, frows.p, fcount.p, rstart.p, gk.p,
+                                                             gw.p, uk.p, uw.p, ucount.p, flag.p); }
+            VG_CHECK_LAUNCH();
+        }
         // segments with more than H_MAXU distinct keys: one global stable sort. Their
         // count, entries and chunks are scanned on the device and read back together.
         DevBuf<int64_t> bigidx(ctx, nc), boff(ctx, nc), cb(ctx, nc), tot(ctx, 4);
