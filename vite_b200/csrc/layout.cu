@@ -104,16 +104,17 @@ __device__ __forceinline__ uint32_t degree_bucket(int64_t d) {
     return d <= 8 ? 0u : d <= 12 ? 1u : d <= 16 ? 2u : d <= 32 ? 3u : 4u;
 }
 
+// (cluster, degree bucket, BFS distance), the distance in dbits bits; unreached
+// vertices (components without a seed) keep their own place, in a bucket of their own
 __global__ void k_order_keys(int64_t nv, const int64_t *__restrict__ rowptr,
                              const int32_t *__restrict__ label, const uint8_t *__restrict__ dist,
-                             uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+                             int dbits, uint64_t *__restrict__ keys, uint32_t *__restrict__ vals) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
          v += (int64_t)gridDim.x * blockDim.x) {
         const int32_t l = label[v];
         const uint64_t b = degree_bucket(rowptr[v + 1] - rowptr[v]);
-        // (cluster, degree bucket, BFS distance); unreached vertices (components
-        // without a seed) keep their own place
-        keys[v] = l < 0 ? ((uint64_t)v << 12) : (((uint64_t)l << 12) | (b << 8) | dist[v]);
+        keys[v] = l < 0 ? (((uint64_t)v << (3 + dbits)) | (7ull << dbits))
+                        : (((uint64_t)l << (3 + dbits)) | (b << dbits) | dist[v]);
         vals[v] = (uint32_t)v;
     }
 }
@@ -315,6 +316,7 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
     { LaunchTimer lt(ctx); k_bfs_init<<<grid, 256, 0, ctx->stream>>>(nv, 0x5eedULL, label.p, dist.p); }
     VG_CHECK_LAUNCH();
     bool done = false;
+    int depth = 0; // largest distance any vertex got
     for (int step0 = 1; step0 <= MAX_BFS_STEPS - 1 && !done; step0 += BFS_GROUP) {
         const int ns = std::min(BFS_GROUP, MAX_BFS_STEPS - step0);
         VG_CUDA(cudaMemsetAsync(claimed.p, 0, BFS_GROUP * sizeof(unsigned long long), ctx->stream));
@@ -326,16 +328,22 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
         }
         VG_CUDA(cudaMemcpyAsync(h, claimed.p, ns * sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
         vg_sync(ctx);
-        for (int k = 0; k < ns; k++) done = done || h[k] == 0;
+        for (int k = 0; k < ns && !done; k++) {
+            if (h[k] == 0) done = true;
+            else depth = step0 + k;
+        }
     }
+    int dbits = 1;
+    while ((1 << dbits) <= depth) dbits++;
     DevBuf<uint64_t> keys(ctx, nv);
     DevBuf<uint32_t> vals(ctx, nv);
     { LaunchTimer lt(ctx);
-      k_order_keys<<<grid, 256, 0, ctx->stream>>>(nv, g->rowptr, label.p, dist.p, keys.p, vals.p); }
+      k_order_keys<<<grid, 256, 0, ctx->stream>>>(nv, g->rowptr, label.p, dist.p, dbits, keys.p,
+                                                  vals.p); }
     VG_CHECK_LAUNCH();
-    int bits = 1;
-    while (bits < 40 && ((int64_t)1 << bits) < nv) bits++;
-    vg_radix_sort_pairs(ctx, keys.p, vals.p, nv, bits + 12);
+    int vbits = 1;
+    while (vbits < 40 && ((int64_t)1 << vbits) < nv) vbits++;
+    vg_radix_sort_pairs(ctx, keys.p, vals.p, nv, vbits + 3 + dbits);
     VG_CUDA(cudaMemcpyAsync(order.p, vals.p, sizeof(int32_t) * nv, cudaMemcpyDeviceToDevice,
                             ctx->stream));
 }
