@@ -284,14 +284,37 @@ def test_rebuild_matches_oracle(ctx, maker):
     assert_graph_equal(g.download(), vo.rebuild(gref, cv))
 
 
+def with_isolated(g, k):
+    """g followed by k vertices without entries"""
+    return vo.Graph(np.concatenate([g.rowptr, np.full(k, g.rowptr[-1], np.int64)]), g.tail,
+                    g.weight)
+
+
+def path_graph(n, seed):
+    rng = np.random.default_rng(seed)
+    a = np.arange(n - 1)
+    w = rng.random(n - 1)
+    return vo._csr_from_list(n, np.concatenate([a, a + 1]), np.concatenate([a + 1, a]),
+                             np.concatenate([w, w]))
+
+
 @pytest.mark.parametrize("layout", [0, 1])
 @pytest.mark.parametrize("case", ["one_community", "blocks_of_600", "random_blocks",
-                                  "ba_blocks_of_12"])
+                                  "ba_blocks_of_12", "isolated_members", "path_blocks_of_300"])
 def test_rebuild_segment_classes(ctx, case, layout):
     """Next-level segments of every size class: the warp hash path (<=256 entries, with
     at most 32 or more distinct neighbours) and the global sorted path (longer), with
-    real weights folded in order."""
-    if case == "ba_blocks_of_12":
+    real weights folded in order. The warp tables read each segment from its members'
+    rows through windows of 32 members: segments of hundreds of short rows slide the
+    window, and members without entries (isolated vertices put into communities by
+    the caller) leave gaps inside it."""
+    if case == "isolated_members":
+        gref = with_isolated(vo.reweight(vo.rgg(16384), 2, 13), 3000)
+        cv = ((np.arange(gref.nv) * 7919) % 250 * 3).astype(np.int64)
+    elif case == "path_blocks_of_300":
+        gref = path_graph(30000, 21)
+        cv = (np.arange(gref.nv) // 300 * 300).astype(np.int64)
+    elif case == "ba_blocks_of_12":
         gref = vo.reweight(vo.ba(20000, 8, 6), 2, 11)
         cv = (np.arange(gref.nv) // 12 * 12).astype(np.int64)
     elif case == "one_community":
