@@ -43,54 +43,105 @@ __global__ void k_bfs_init(int64_t nv, uint64_t seed, int32_t *__restrict__ labe
 }
 
 // one level: vertices at distance step-1 claim their unlabeled neighbours. A warp
-// takes 32 consecutive vertices and walks the frontier rows among them four at a
-// time, eight lanes to a row, so a row's claims are issued together instead of as
-// a chain of dependent loads and compare-and-swaps.
+// takes 128 consecutive vertices (four per lane, read as one word of distances),
+// lists its frontier vertices in shared memory and spreads all their entries over
+// its lanes, four per lane per pass (each lane finds its entry's row by a search
+// over the rows' running offsets): the tail loads, distance gathers and claims of a
+// whole pass are issued together, so a pass costs one chain of dependent memory
+// accesses for up to 128 entries.
 // unvisited vertices are found through the byte array of distances (255 =
 // unvisited), which stays in L2; the label's compare-and-swap settles races
-__device__ __forceinline__ unsigned long long bfs_claim(const int32_t *__restrict__ tail, int64_t e,
-                                                        int32_t lu, int step,
-                                                        int32_t *__restrict__ label,
-                                                        uint8_t *__restrict__ dist) {
-    const int32_t w = tail[e];
-    if (dist[w] == 255 && atomicCAS(&label[w], -1, lu) == -1) {
-        dist[w] = (uint8_t)step;
-        return 1;
-    }
-    return 0;
-}
+constexpr int BFS_WARPS = 8;
 
-__global__ void k_bfs_step(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail,
-                           int64_t nv, int step, int32_t *__restrict__ label,
-                           uint8_t *__restrict__ dist, unsigned long long *__restrict__ claimed) {
+__global__ void __launch_bounds__(BFS_WARPS * 32) k_bfs_step(
+    const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail, int64_t nv, int step,
+    int32_t *__restrict__ label, uint8_t *__restrict__ dist, unsigned long long *__restrict__ claimed) {
+    __shared__ int32_t fl_all[BFS_WARPS][128];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    int32_t *fl = fl_all[threadIdx.x >> 5];
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t prev = (uint32_t)(step - 1);
     unsigned long long mine = 0;
-    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < nv;
-         base += nw * 32) {
-        const int64_t u = base + lane;
-        const bool front = u < nv && dist[u] == step - 1;
-        int64_t e0 = 0, e1 = 0;
-        int32_t lu = -1;
-        if (front) {
-            e0 = rowptr[u];
-            e1 = rowptr[u + 1];
-            lu = label[u];
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 128; base < nv;
+         base += nw * 128) {
+        // 1. the frontier among vertices u0 .. u0 + 3 (u0 is a multiple of 4)
+        const int64_t u0 = base + 4 * lane;
+        unsigned fb = 0;
+        if (u0 + 3 < nv) {
+            const uint32_t dw = *reinterpret_cast<const uint32_t *>(dist + u0);
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (((dw >> (8 * q)) & 0xffu) == prev) fb |= 1u << q;
+        } else {
+            for (int q = 0; q < 4; q++)
+                if (u0 + q < nv && dist[u0 + q] == prev) fb |= 1u << q;
         }
-        // four groups of eight lanes: in round k, group g walks the row of the
-        // (4k + g)-th frontier vertex of the window (rounds are warp-uniform)
-        const unsigned fm = __ballot_sync(full, front);
-        const int nf = __popc(fm), grp = lane >> 3, sub = lane & 7;
-        for (int k = 0; 4 * k < nf; k++) {
-            const int r = 4 * k + grp;
-            const bool has = r < nf;
-            const int src = has ? (int)__fns(fm, 0, r + 1) : 0;
-            const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
-            const int32_t L = __shfl_sync(full, lu, src);
-            if (has)
-                for (int64_t e = E0 + sub; e < E1; e += 8) mine += bfs_claim(tail, e, L, step, label, dist);
+        const int cnt = __popc(fb);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(full, incl, o);
+            if (lane >= o) incl += y;
         }
+        const int total = __shfl_sync(full, incl, 31);
+        if (total == 0) continue;
+        {
+            int at = incl - cnt;
+            for (int q = 0; q < 4; q++)
+                if ((fb >> q) & 1u) fl[at++] = (int32_t)(u0 + q);
+        }
+        __syncwarp();
+        // 2. up to 32 frontier vertices at a time, their entries spread over the lanes
+        for (int r0 = 0; r0 < total; r0 += 32) {
+            const bool has = r0 + lane < total;
+            int64_t e0 = 0, len = 0;
+            int32_t lu = 0;
+            if (has) {
+                const int32_t u = fl[r0 + lane];
+                e0 = rowptr[u];
+                len = rowptr[u + 1] - e0;
+                lu = label[u];
+            }
+            int64_t ri = len; // inclusive running offsets of the rows
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t y = __shfl_up_sync(full, ri, o);
+                if (lane >= o) ri += y;
+            }
+            const int64_t T = __shfl_sync(full, ri, 31);
+            const int64_t rs = has ? ri - len : INT64_MAX; // this lane's row start
+            for (int64_t k0 = 0; k0 < T; k0 += 128) {
+                int32_t w[4], L[4];
+                bool h[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int64_t k = k0 + 32 * q + lane;
+                    h[q] = k < T;
+                    const int64_t kq = h[q] ? k : 0;
+                    // the row holding entry kq: the last lane whose row starts at or before it
+                    int j = 0;
+#pragma unroll
+                    for (int st = 16; st; st >>= 1) {
+                        const int64_t r = __shfl_sync(full, rs, j + st);
+                        if (r <= kq) j += st;
+                    }
+                    const int64_t ej = __shfl_sync(full, e0, j) + (kq - __shfl_sync(full, rs, j));
+                    L[q] = __shfl_sync(full, lu, j);
+                    w[q] = h[q] ? tail[ej] : 0;
+                }
+                uint8_t dd[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) dd[q] = h[q] ? dist[w[q]] : 0;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (h[q] && dd[q] == 255 && atomicCAS(&label[w[q]], -1, L[q]) == -1) {
+                        dist[w[q]] = (uint8_t)step;
+                        mine++;
+                    }
+            }
+        }
+        __syncwarp();
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, o);
@@ -313,6 +364,7 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
     unsigned long long *h =
         (unsigned long long *)vg_pinned(ctx, BFS_GROUP * sizeof(unsigned long long));
     const int grid = vg_grid(ctx, nv, 256);
+    const int sgrid = vg_grid(ctx, (nv + 3) / 4, BFS_WARPS * 32); // a lane per four vertices
     { LaunchTimer lt(ctx); k_bfs_init<<<grid, 256, 0, ctx->stream>>>(nv, 0x5eedULL, label.p, dist.p); }
     VG_CHECK_LAUNCH();
     bool done = false;
@@ -322,8 +374,8 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
         VG_CUDA(cudaMemsetAsync(claimed.p, 0, BFS_GROUP * sizeof(unsigned long long), ctx->stream));
         for (int k = 0; k < ns; k++) {
             LaunchTimer lt(ctx);
-            k_bfs_step<<<grid, 256, 0, ctx->stream>>>(g->rowptr, g->tail, nv, step0 + k, label.p,
-                                                      dist.p, claimed.p + k);
+            k_bfs_step<<<sgrid, BFS_WARPS * 32, 0, ctx->stream>>>(g->rowptr, g->tail, nv, step0 + k,
+                                                                 label.p, dist.p, claimed.p + k);
             VG_CHECK_LAUNCH();
         }
         VG_CUDA(cudaMemcpyAsync(h, claimed.p, ns * sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
