@@ -186,9 +186,9 @@ vg_status vg_vertex_degree(vg_ctx *ctx, vg_graph *g, double *vdeg_out, double *c
  * reduction is a file-scope device array of 512 KiB held by every GPU that loads the
  * library: at most VG_NOALLOC_MAX_VERTICES vertices, larger graphs are rejected with
  * VG_ERR_ARG. All calls share that array, so calls that overlap on the GPU race. The
- * first call on a device looks the array's address up with that device current; make
- * it before any stream capture. The address is kept for the life of the process, so
- * do not call this function again on a device after cudaDeviceReset. errbuf (may be
+ * first call on a device looks the array's address up with that device current. The
+ * address is kept for the life of the process, so do not call this function again on
+ * a device after cudaDeviceReset. errbuf (may be
  * NULL) receives a message on failure. Allocates nothing: no cudaMalloc, no
  * cudaFree. */
 #define VG_NOALLOC_MAX_VERTICES (2048LL * 65536LL)
