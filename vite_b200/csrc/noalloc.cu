@@ -15,9 +15,8 @@
 //     streams, two host threads) race on it and must be serialised by the caller;
 //   * the first call on a device looks up the array's device address with that
 //     device current (cudaGetSymbolAddress). The address is kept for the life of
-//     the process: a
-//     cudaDeviceReset would leave it stale, so the entry point must not be used on
-//     a device after a reset;
+//     the process: a cudaDeviceReset would leave it stale, so the entry point must
+//     not be used on a device after a reset;
 //   * the row offsets are not checked (checking them would need memory of its
 //     own): the caller passes a valid CSR, offsets non-decreasing and inside the
 //     weights array.
