@@ -61,35 +61,41 @@ __global__ void k_row_starts(const uint64_t *__restrict__ keys, const int64_t *_
 // (hubs, giant communities) are cut into chunks of COPY_CHUNK entries, one block per
 // chunk, so one row never serialises a warp.
 constexpr int64_t LONG_ROW = 4096;
+// a copy takes a warp per row instead of eight lanes when rows average this many
+// entries
+constexpr int64_t LANES32_ROW = 64;
 constexpr int64_t COPY_CHUNK = 4096;
 
 // vertices in grouped order: each one's row goes to its segment, neighbours renamed
 // to their ordering keys
+// G lanes per row: 8 for rows of a few tens of entries, 32 when the rows are long
+// (a coarse level with hundreds of entries per row)
+template <int G>
 __global__ void k_group_copy(const int32_t *__restrict__ tail, const double *__restrict__ w,
                              const int64_t *__restrict__ src_start, const int64_t *__restrict__ off,
                              int64_t nv, const int32_t *__restrict__ new_key,
                              int32_t *__restrict__ gk, double *__restrict__ gw) {
-    const int sub = threadIdx.x & 7;
-    const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
-    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
+    const int sub = threadIdx.x & (G - 1);
+    const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) / G;
     for (int64_t k = grp; k < nv; k += ng) {
         const int64_t o = off[k], len = off[k + 1] - o;
         if (len > LONG_ROW) continue;
         const int64_t e0 = src_start[k];
         // two entries per lane per step: both tails are loaded before the key gathers
-        for (int64_t j = sub; j < len; j += 16) {
-            const bool two = j + 8 < len;
+        for (int64_t j = sub; j < len; j += 2 * G) {
+            const bool two = j + G < len;
             const int32_t t0 = tail[e0 + j];
-            const int32_t t1 = two ? tail[e0 + j + 8] : 0;
+            const int32_t t1 = two ? tail[e0 + j + G] : 0;
             const double w0 = w[e0 + j];
-            const double w1 = two ? w[e0 + j + 8] : 0.0;
+            const double w1 = two ? w[e0 + j + G] : 0.0;
             const int32_t k0 = new_key[t0];
             const int32_t k1 = two ? new_key[t1] : 0;
             gk[o + j] = k0;
             gw[o + j] = w0;
             if (two) {
-                gk[o + j + 8] = k1;
-                gw[o + j + 8] = w1;
+                gk[o + j + G] = k1;
+                gw[o + j + G] = w1;
             }
         }
     }
@@ -540,17 +546,18 @@ __global__ void k_big_counts(int64_t nbig, const int32_t *__restrict__ big_row,
         ucount[big_row[q]] = (q + 1 < nbig ? rowfirst[q + 1] : heads) - rowfirst[q];
 }
 
+template <int G> // lanes per row, as k_group_copy
 __global__ void k_compact_rows(int64_t nc, const int64_t *__restrict__ rstart,
                                const int64_t *__restrict__ rowptr, const int32_t *__restrict__ uk,
                                const double *__restrict__ uw, const int32_t *__restrict__ key_to_pos,
                                int32_t *__restrict__ tail, double *__restrict__ w) {
-    const int sub = threadIdx.x & 7;
-    const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
-    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
+    const int sub = threadIdx.x & (G - 1);
+    const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) / G;
     for (int64_t row = grp; row < nc; row += ng) {
         const int64_t s = rstart[row], o = rowptr[row], len = rowptr[row + 1] - o;
         if (len > LONG_ROW) continue;
-        for (int64_t j = sub; j < len; j += 8) {
+        for (int64_t j = sub; j < len; j += G) {
             const int32_t k = uk[s + j];
             tail[o + j] = key_to_pos ? key_to_pos[k] : k;
             w[o + j] = uw[s + j];
@@ -661,8 +668,12 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     DevBuf<double> gw(ctx, ne);
     if (ne) {
         LaunchTimer lt(ctx);
-        k_group_copy<<<vg_grid(ctx, nv * 8, 256), 256, 0, ctx->stream>>>(
-            g->tail, g->weight, src_start.p, off.p, nv, new_key, gk.p, gw.p);
+        if (ne >= LANES32_ROW * nv)
+            k_group_copy<32><<<vg_grid(ctx, nv * 32, 256), 256, 0, ctx->stream>>>(
+                g->tail, g->weight, src_start.p, off.p, nv, new_key, gk.p, gw.p);
+        else
+            k_group_copy<8><<<vg_grid(ctx, nv * 8, 256), 256, 0, ctx->stream>>>(
+                g->tail, g->weight, src_start.p, off.p, nv, new_key, gk.p, gw.p);
     }
     VG_CHECK_LAUNCH();
     {
@@ -791,8 +802,12 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
     DevBuf<double> w(ctx, m);
     if (nc) {
         LaunchTimer lt(ctx);
-        k_compact_rows<<<vg_grid(ctx, nc * 8, 256), 256, 0, ctx->stream>>>(
-            nc, rstart.p, ucount.p, uk.p, uw.p, key_to_pos, tail.p, w.p);
+        if (m >= LANES32_ROW * nc)
+            k_compact_rows<32><<<vg_grid(ctx, nc * 32, 256), 256, 0, ctx->stream>>>(
+                nc, rstart.p, ucount.p, uk.p, uw.p, key_to_pos, tail.p, w.p);
+        else
+            k_compact_rows<8><<<vg_grid(ctx, nc * 8, 256), 256, 0, ctx->stream>>>(
+                nc, rstart.p, ucount.p, uk.p, uw.p, key_to_pos, tail.p, w.p);
     }
     VG_CHECK_LAUNCH();
     {
