@@ -44,6 +44,9 @@ constexpr int TB = 256;
 #ifndef VG_WS_GRID
 #define VG_WS_GRID 4 // CTAs per SM in the grids of the warp kernels
 #endif
+#ifndef VG_CT_GRID_S
+#define VG_CT_GRID_S 8 // CTAs per SM in the grid of the CTA kernel's small table
+#endif
 #ifndef VG_CT_GRID
 #define VG_CT_GRID 2 // CTAs per SM in the grid of the CTA kernel
 #endif
@@ -62,6 +65,7 @@ constexpr int WT_WARPS = 4;
 static_assert(2 * WS_MAXDEG <= WS_CAP && 2 * WT_MAXDEG <= WT_CAP, "warp tables too small");
 constexpr int CT_MAXDEG = VG_CT_MAXDEG;
 constexpr int CT_CAP = 8192;
+constexpr int CT_CAP_S = 2048;
 constexpr int CT_THREADS = 256;
 constexpr int32_t EMPTY = -1;
 
@@ -855,6 +859,10 @@ struct CtaShared {
     double counter0;
 };
 
+// CAP: the table's slots. The class runs as two launches over the same list, a
+// table of CT_CAP_S slots for the rows of at most CT_CAP_S / 2 entries (more CTAs fit
+// per SM) and one of CT_CAP slots for the longer ones; each skips the other's rows.
+template <int CAP>
 __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int32_t *__restrict__ list,
                                                           int64_t count) {
     extern __shared__ unsigned char smem_raw[];
@@ -863,9 +871,12 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
     double *vals = reinterpret_cast<double *>(smem_raw);
-    int32_t *keys = reinterpret_cast<int32_t *>(vals + CT_CAP);
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + CAP);
     for (int64_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
         const int32_t v = list[idx];
+        const int64_t e0 = a.rowptr[v];
+        const int64_t d = a.rowptr[v + 1] - e0;
+        if ((CAP == CT_CAP) != (d > CT_CAP_S / 2)) continue; // the other launch's row
         double cst;
         if (!vertex_live(a, v, cst)) continue;
         const int32_t cc = a.curr[v];
@@ -873,8 +884,6 @@ __global__ void __launch_bounds__(CT_THREADS) k_sweep_cta(SweepArgs a, const int
             if (threadIdx.x == 0) a.cw[v] = a.frozen[v];
             continue;
         }
-        const int64_t e0 = a.rowptr[v];
-        const int64_t d = a.rowptr[v + 1] - e0;
         int logcap = 5;
         while (((int64_t)1 << logcap) < 2 * d) logcap++;
         const int64_t cap = (int64_t)1 << logcap;
@@ -1906,7 +1915,7 @@ static void build_buckets(vg_ctx *ctx, const vg_graph *g, const int32_t *colors,
     vg_sync(ctx); // keep `fill` alive until the copy is done
 }
 
-static size_t cta_smem_bytes() { return (size_t)CT_CAP * (sizeof(double) + sizeof(int32_t)); }
+static size_t cta_smem_bytes(int cap = CT_CAP) { return (size_t)cap * (sizeof(double) + sizeof(int32_t)); }
 
 static void configure_kernels_once() {
     static bool done = false;
@@ -1917,8 +1926,10 @@ static void configure_kernels_once() {
     VG_CUDA(cudaFuncSetAttribute(k_sweep_warp<WT_CAP, WT_WARPS>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)warp_smem_bytes<WT_CAP, WT_WARPS>()));
-    VG_CUDA(cudaFuncSetAttribute(k_sweep_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    VG_CUDA(cudaFuncSetAttribute(k_sweep_cta<CT_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_smem_bytes()));
+    VG_CUDA(cudaFuncSetAttribute(k_sweep_cta<CT_CAP_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_smem_bytes(CT_CAP_S)));
     done = true;
 }
 
@@ -2080,8 +2091,14 @@ static void sweep_color(vg_ctx *ctx, const SweepArgs &a, const Buckets &b, int64
                 a, list + s, n);
             break;
         case 4:
-            k_sweep_cta<<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, VG_CT_GRID), CT_THREADS, cta_smem_bytes(),
-                          st>>>(a, list + s, n);
+            k_sweep_cta<CT_CAP_S><<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, VG_CT_GRID_S), CT_THREADS,
+                                    cta_smem_bytes(CT_CAP_S), st>>>(a, list + s, n);
+            VG_CHECK_LAUNCH();
+            if (effective_tuning(ctx).ct_max > CT_CAP_S / 2) {
+                LaunchTimer lt2(ctx);
+                k_sweep_cta<CT_CAP><<<vg_grid(ctx, n * CT_THREADS, CT_THREADS, VG_CT_GRID), CT_THREADS,
+                                      cta_smem_bytes(), st>>>(a, list + s, n);
+            }
             break;
         default:
             break;
