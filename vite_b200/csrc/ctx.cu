@@ -329,20 +329,54 @@ extern "C" vg_status vg_graph_upload(vg_ctx *ctx, int64_t nv, int64_t ne, const 
         VG_CUDA(cudaMemsetAsync(bad.p, 0, 2 * sizeof(int), ctx->stream));
         vg_check_rowptr_async(ctx, rp.p, nv + 1, 0, ne, bad.p);
         if (ne) {
-            // stage the 16-byte records through a bounded device buffer in chunks
+            // stage the 16-byte records through two bounded device buffers in chunks:
+            // the copies run back to back on the context's stream while the side
+            // stream splits the chunk before (a buffer is refilled only after its split)
             const int64_t chunk = ne < (int64_t)(1 << 24) ? ne : (int64_t)(1 << 24);
-            DevBuf<vg_edge> stage(ctx, chunk);
-            for (int64_t off = 0; off < ne; off += chunk) {
-                const int64_t len = (ne - off) < chunk ? (ne - off) : chunk;
-                VG_CUDA(cudaMemcpyAsync(stage.p, edges + off, sizeof(vg_edge) * len,
-                                        cudaMemcpyHostToDevice, ctx->stream));
-                {
-                    LaunchTimer lt(ctx);
-                    k_split_edges<<<vg_grid(ctx, len, 256), 256, 0, ctx->stream>>>(
-                        stage.p, len, nv, tail.p + off, w.p + off, bad.p + 1);
+            DevBuf<vg_edge> stage0(ctx, chunk), stage1(ctx, chunk);
+            vg_edge *stage[2] = {stage0.p, stage1.p};
+            cudaEvent_t copied[2] = {nullptr, nullptr}, split[2] = {nullptr, nullptr};
+            auto destroy = [&] {
+                for (int b = 0; b < 2; b++) {
+                    if (copied[b]) cudaEventDestroy(copied[b]);
+                    if (split[b]) cudaEventDestroy(split[b]);
                 }
-                VG_CHECK_LAUNCH();
+            };
+            try {
+                for (int b = 0; b < 2; b++) {
+                    VG_CUDA(cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming));
+                    VG_CUDA(cudaEventCreateWithFlags(&split[b], cudaEventDisableTiming));
+                }
+                const bool two = !ctx->profile; // with profiling every launch stays on one stream
+                cudaStream_t ss = two ? ctx->side : ctx->stream;
+                int64_t k = 0;
+                for (int64_t off = 0; off < ne; off += chunk, k++) {
+                    const int b = (int)(k & 1);
+                    const int64_t len = (ne - off) < chunk ? (ne - off) : chunk;
+                    if (two && k >= 2) VG_CUDA(cudaStreamWaitEvent(ctx->stream, split[b], 0));
+                    VG_CUDA(cudaMemcpyAsync(stage[b], edges + off, sizeof(vg_edge) * len,
+                                            cudaMemcpyHostToDevice, ctx->stream));
+                    if (two) {
+                        VG_CUDA(cudaEventRecord(copied[b], ctx->stream));
+                        VG_CUDA(cudaStreamWaitEvent(ss, copied[b], 0));
+                    }
+                    {
+                        LaunchTimer lt(ctx);
+                        k_split_edges<<<vg_grid(ctx, len, 256), 256, 0, ss>>>(
+                            stage[b], len, nv, tail.p + off, w.p + off, bad.p + 1);
+                    }
+                    VG_CHECK_LAUNCH();
+                    if (two) VG_CUDA(cudaEventRecord(split[b], ss));
+                }
+                if (two) { // the stream waits for the last splits
+                    for (int b = 0; b < 2 && b < k; b++)
+                        VG_CUDA(cudaStreamWaitEvent(ctx->stream, split[(k - 1 - b) & 1], 0));
+                }
+            } catch (...) {
+                destroy();
+                throw;
             }
+            destroy();
         }
         int *hb = (int *)vg_pinned(ctx, 2 * sizeof(int));
         VG_CUDA(cudaMemcpyAsync(hb, bad.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
