@@ -1327,20 +1327,86 @@ __device__ __forceinline__ double row_fold(const double *__restrict__ w, int64_t
     return sum;
 }
 
+// With integral weights, rows longer than DEG_HUGE (the hubs of a coarse level) are
+// cut into DEG_CHUNK-entry chunks summed by many blocks (exact partial sums, added
+// atomically), so one row does not hold the whole launch on one warp.
+constexpr int64_t DEG_HUGE = 16384;
+constexpr int64_t DEG_CHUNK = 16384;
+
 // one lane per row for rows of at most DEG_LONG entries; longer rows are listed
-// (any order) for k_degree_long
+// (any order) for k_degree_long, or for the chunked sums when integral and huge
+// (their degree starts at zero)
 __global__ void k_degree(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
                          int64_t nv, double *__restrict__ vdeg, int32_t *__restrict__ long_rows,
-                         int64_t long_cap, unsigned long long *__restrict__ long_count) {
+                         int64_t long_cap, unsigned long long *__restrict__ long_count,
+                         int32_t *__restrict__ huge_rows, int64_t huge_cap,
+                         unsigned long long *__restrict__ huge_count) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
          v += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e0 = rowptr[v], e1 = rowptr[v + 1];
         if (e1 - e0 <= DEG_LONG) {
             vdeg[v] = row_fold(w, e0, e1);
+        } else if (huge_rows && e1 - e0 > DEG_HUGE) {
+            vdeg[v] = 0.0;
+            const unsigned long long s = atomicAdd(huge_count, 1ULL);
+            if ((int64_t)s < huge_cap) huge_rows[s] = (int32_t)v;
         } else {
             const unsigned long long s = atomicAdd(long_count, 1ULL);
             if ((int64_t)s < long_cap) long_rows[s] = (int32_t)v;
         }
+    }
+}
+
+// exclusive prefix of the listed huge rows' chunk counts (one thread; the list holds
+// at most ne / DEG_HUGE rows); cb[n] = all chunks
+__global__ void k_degree_huge_plan(const int64_t *__restrict__ rowptr,
+                                   const int32_t *__restrict__ huge_rows, int64_t huge_cap,
+                                   const unsigned long long *__restrict__ huge_count,
+                                   int64_t *__restrict__ cb) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int64_t n = min((int64_t)*huge_count, huge_cap);
+    int64_t run = 0;
+    for (int64_t q = 0; q < n; q++) {
+        cb[q] = run;
+        const int32_t v = huge_rows[q];
+        run += (rowptr[v + 1] - rowptr[v] + DEG_CHUNK - 1) / DEG_CHUNK;
+    }
+    cb[n] = run;
+}
+
+// one block per chunk of a huge row: eight loads per thread issued before the adds,
+// a warp tree, and one atomic per warp (every partial sum an exact integer)
+__global__ void k_degree_huge(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
+                              double *__restrict__ vdeg, const int32_t *__restrict__ huge_rows,
+                              int64_t huge_cap, const unsigned long long *__restrict__ huge_count,
+                              const int64_t *__restrict__ cb) {
+    const int64_t n = min((int64_t)*huge_count, huge_cap);
+    const int64_t nch = cb[n];
+    for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+        int64_t lo = 0, hi = n; // the largest q with cb[q] <= c
+        while (hi - lo > 1) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (cb[mid] <= c) lo = mid;
+            else hi = mid;
+        }
+        const int32_t v = huge_rows[lo];
+        const int64_t E1 = rowptr[v + 1];
+        const int64_t a0 = rowptr[v] + (c - cb[lo]) * DEG_CHUNK;
+        const int64_t a1 = min(a0 + DEG_CHUNK, E1);
+        double sum = 0.0;
+        for (int64_t k0 = a0 + threadIdx.x; k0 < a1; k0 += 8 * (int64_t)blockDim.x) {
+            double x[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                const int64_t k = k0 + (int64_t)t * blockDim.x;
+                x[t] = k < a1 ? w[k] : 0.0;
+            }
+#pragma unroll
+            for (int t = 0; t < 8; t++) sum = __dadd_rn(sum, x[t]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum = __dadd_rn(sum, __shfl_xor_sync(0xffffffffu, sum, o));
+        if ((threadIdx.x & 31) == 0 && sum != 0.0) atomicAdd(&vdeg[v], sum);
     }
 }
 
@@ -1940,14 +2006,29 @@ static void vertex_degrees(vg_ctx *ctx, const vg_graph *g, double *vdeg, int int
     if (nv == 0) return;
     const int64_t cap = std::min<int64_t>(nv, g->ne / (DEG_LONG + 1) + 1);
     DevBuf<int32_t> list(ctx, cap);
-    DevBuf<unsigned long long> cnt(ctx, 1);
-    VG_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), ctx->stream));
+    DevBuf<unsigned long long> cnt(ctx, 2); // long rows, huge rows
+    VG_CUDA(cudaMemsetAsync(cnt.p, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    const bool chunked = integral && g->ne > DEG_HUGE;
+    const int64_t hcap = chunked ? std::min<int64_t>(nv, g->ne / (DEG_HUGE + 1) + 1) : 0;
+    DevBuf<int32_t> hlist(ctx, hcap);
+    DevBuf<int64_t> hcb(ctx, chunked ? hcap + 1 : 0);
     {
         LaunchTimer lt(ctx);
         k_degree<<<vg_grid(ctx, nv, 256), 256, 0, ctx->stream>>>(g->rowptr, g->weight, nv, vdeg,
-                                                                 list.p, cap, cnt.p);
+                                                                 list.p, cap, cnt.p, hlist.p, hcap,
+                                                                 cnt.p + 1);
     }
     VG_CHECK_LAUNCH();
+    if (chunked) {
+        { LaunchTimer lt(ctx);
+          k_degree_huge_plan<<<1, 32, 0, ctx->stream>>>(g->rowptr, hlist.p, hcap, cnt.p + 1, hcb.p); }
+        VG_CHECK_LAUNCH();
+        { LaunchTimer lt(ctx);
+          k_degree_huge<<<(int)std::min<int64_t>(g->ne / DEG_CHUNK + hcap, 16LL * ctx->sm_count), 256,
+                          0, ctx->stream>>>(g->rowptr, g->weight, vdeg, hlist.p, hcap, cnt.p + 1,
+                                            hcb.p); }
+        VG_CHECK_LAUNCH();
+    }
     if (g->ne > DEG_LONG) {
         LaunchTimer lt(ctx);
         k_degree_long<<<vg_grid(ctx, cap * 32, 256, 8), 256, 0, ctx->stream>>>(
