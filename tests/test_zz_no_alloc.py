@@ -21,11 +21,18 @@ def test_rejects_sizes_beyond_the_maximum():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("maker", ["rgg_distance", "ba_unit"])
+@pytest.mark.parametrize("maker", ["rgg_distance", "ba_unit", "ba_real"])
 def test_noalloc_matches_vg_vertex_degree(maker):
+    """ba_*: hub rows of hundreds to thousands of entries, which the warp folds
+    together; with real weights their sums must keep the serial CSR order"""
     import torch
 
-    g = vo.rgg(65536) if maker == "rgg_distance" else vo.ba(20000, 8, 3)
+    if maker == "rgg_distance":
+        g = vo.rgg(65536)
+    elif maker == "ba_unit":
+        g = vo.ba(20000, 8, 3)
+    else:
+        g = vo.reweight(vo.ba(20000, 8, 3), 2, 7)
     with vite_b200.Context(0) as ctx:
         vd_ref, c_ref = ctx.vertex_degree(ctx.upload(g.rowptr, g.tail, g.weight))
     rp = torch.tensor(g.rowptr, dtype=torch.int64, device="cuda")

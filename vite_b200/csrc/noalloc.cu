@@ -53,24 +53,55 @@ __device__ double na_block_sum(double v, double *ws) {
     return s;
 }
 
+// rows longer than this are folded by the whole warp
+constexpr int64_t NA_LONG = 64;
+
 // one block per tile: each row summed in CSR order (as distSumVertexDegree), and
-// the tile's degrees reduced into its partial
+// the tile's degrees reduced into its partial. A lane folds its own row when it is
+// short; the warp's long rows (hubs) are folded one after another by all its lanes,
+// 32 consecutive weights loaded at a time and added in lane order from broadcasts,
+// so every lane holds the serial fold's bits and a hub costs its length / 32 steps
 __global__ void __launch_bounds__(NA_THREADS) k_na_degree(const int64_t *__restrict__ rowptr,
                                                           const double *__restrict__ w, int64_t nv,
                                                           double *__restrict__ vdeg,
                                                           double *__restrict__ partial) {
     __shared__ double ws[32];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     double s = 0.0;
     const int64_t base = (int64_t)blockIdx.x * NA_TILE;
-    for (int k = threadIdx.x; k < NA_TILE; k += NA_THREADS) {
+    for (int k = threadIdx.x; k < NA_TILE; k += NA_THREADS) { // warp-uniform trip count
         const int64_t v = base + k;
-        if (v >= nv) break;
+        const bool valid = v < nv;
+        int64_t e0 = 0, e1 = 0;
+        if (valid) {
+            e0 = rowptr[v];
+            e1 = rowptr[v + 1];
+        }
+        // w is null only for a CSR without entries (checked on the host)
+        const bool lng = valid && w && e1 - e0 > NA_LONG;
         double tw = 0.0;
-        const int64_t e1 = rowptr[v + 1];
-        if (w) // null only for a CSR without entries (checked on the host)
-            for (int64_t e = rowptr[v]; e < e1; e++) tw = __dadd_rn(tw, w[e]);
-        vdeg[v] = tw;
-        s = __dadd_rn(s, tw);
+        if (valid && w && !lng)
+            for (int64_t e = e0; e < e1; e++) tw = __dadd_rn(tw, w[e]);
+        for (unsigned lm = __ballot_sync(full, lng); lm; lm &= lm - 1) {
+            const int src = __ffs(lm) - 1;
+            const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
+            double acc = 0.0;
+            for (int64_t b = E0; b < E1; b += 32) {
+                const double x = b + lane < E1 ? w[b + lane] : 0.0;
+                const int cnt = (int)min((int64_t)32, E1 - b);
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const double y = __shfl_sync(full, x, j);
+                    if (j < cnt) acc = __dadd_rn(acc, y);
+                }
+            }
+            if (lane == src) tw = acc;
+        }
+        if (valid) {
+            vdeg[v] = tw;
+            s = __dadd_rn(s, tw);
+        }
     }
     s = na_block_sum(s, ws);
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
