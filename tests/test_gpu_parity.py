@@ -94,12 +94,18 @@ def test_upload_download_roundtrip(ctx):
 # --------------------------------------------------------------------------------------
 # operators
 
-@pytest.mark.parametrize("maker", ["rgg", "ba", "hub"])
+@pytest.mark.parametrize("maker", ["rgg", "ba", "hub", "star_big", "star_big_real"])
 def test_vertex_degree(ctx, maker):
+    """star_big: a 40,000-entry hub row, which integral weights sum in chunks over many
+    blocks (and real weights as one ordered fold)"""
     if maker == "rgg":
         ref = vo.rgg(65536)
     elif maker == "ba":
         ref = vo.ba(20000, 8, 3)
+    elif maker == "star_big":
+        ref = star_graph(40001, 3.0)
+    elif maker == "star_big_real":
+        ref = vo.reweight(star_graph(40001), 2, 17)
     else:
         ref = star_graph(9000)
     vd, c = ctx.vertex_degree(upload(ctx, ref))
