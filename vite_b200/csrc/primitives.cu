@@ -169,13 +169,22 @@ void vg_scan_i32_async(vg_ctx *ctx, const int32_t *in, int64_t *out, int64_t n,
 }
 // ---------------------------------------------------------------------------------
 // stable LSD radix sort, 8-bit digits
+//
+// One pass = a per-tile digit histogram, a scan of the (digit, tile) counts, and a
+// scatter. A tile is RS_TILE consecutive elements; each of its warps ranks its own
+// run of 32 * RS_ROUNDS elements in order (32 elements per round, equal digits ranked
+// by lane through match_any), so the tile-local order of equal digits is the input
+// order and the sort is stable. The scatter first places the tile in digit order in
+// shared memory and then writes it out with consecutive threads on consecutive
+// elements, so each digit's run leaves the tile as whole coalesced stores instead of
+// one partial sector per element.
 
 namespace {
 
 constexpr int RS_BLOCK = 256;
-constexpr int RS_ROUNDS = 8;
-constexpr int RS_TILE = RS_BLOCK * RS_ROUNDS;
 constexpr int RS_WARPS = RS_BLOCK / 32;
+constexpr int RS_ROUNDS = 16; // rounds of 32 elements per warp
+constexpr int RS_TILE = RS_BLOCK * RS_ROUNDS;
 
 __global__ void k_radix_hist(const uint64_t *__restrict__ keys, int64_t n, int shift,
                              int32_t *__restrict__ counts, int64_t ntiles) {
@@ -183,7 +192,7 @@ __global__ void k_radix_hist(const uint64_t *__restrict__ keys, int64_t n, int s
     hist[threadIdx.x] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * RS_TILE;
-#pragma unroll
+#pragma unroll 4
     for (int r = 0; r < RS_ROUNDS; r++) {
         const int64_t i = base + (int64_t)r * RS_BLOCK + threadIdx.x;
         if (i < n) atomicAdd(&hist[(keys[i] >> shift) & 0xff], 1);
@@ -192,52 +201,86 @@ __global__ void k_radix_hist(const uint64_t *__restrict__ keys, int64_t n, int s
     counts[(int64_t)threadIdx.x * ntiles + blockIdx.x] = hist[threadIdx.x];
 }
 
-// element order inside a tile is (round, thread); ranks preserve it, so the sort is stable
-__global__ void k_radix_scatter(const uint64_t *__restrict__ kin, const uint32_t *__restrict__ vin,
-                                uint64_t *__restrict__ kout, uint32_t *__restrict__ vout, int64_t n,
-                                int shift, const int64_t *__restrict__ offsets, int64_t ntiles) {
-    __shared__ int64_t digit_base[256];
-    __shared__ int32_t warp_cnt[RS_WARPS][256];
+struct RadixSmem {
+    uint64_t sk[RS_TILE];
+    uint32_t sv[RS_TILE];
+    int32_t warp_cnt[RS_WARPS][256]; // per warp: digit counts, then exclusive prefix over warps
+    int64_t digit_base[256];         // where the tile's run of each digit starts in the output
+    int32_t tile_start[256];         // where it starts inside the tile's sorted order
+    int32_t wsum[RS_WARPS];
+};
+
+__global__ void __launch_bounds__(RS_BLOCK) k_radix_scatter(
+    const uint64_t *__restrict__ kin, const uint32_t *__restrict__ vin, uint64_t *__restrict__ kout,
+    uint32_t *__restrict__ vout, int64_t n, int shift, const int64_t *__restrict__ offsets,
+    int64_t ntiles) {
+    extern __shared__ unsigned char rs_raw[];
+    RadixSmem &S = *reinterpret_cast<RadixSmem *>(rs_raw);
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    digit_base[threadIdx.x] = offsets[(int64_t)threadIdx.x * ntiles + blockIdx.x];
-    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
     const unsigned lt_mask = (1u << lane) - 1u;
+    const int64_t tile0 = (int64_t)blockIdx.x * RS_TILE;
+    const int64_t base = tile0 + (int64_t)warp * (32 * RS_ROUNDS);
+    for (int d = lane; d < 256; d += 32) S.warp_cnt[warp][d] = 0;
+    S.digit_base[threadIdx.x] = offsets[(int64_t)threadIdx.x * ntiles + blockIdx.x];
+    __syncwarp();
+    // 1. each warp ranks its run: loc = earlier elements of the run with the same
+    // digit; the run goes to shared memory in input order meanwhile
+    int loc[RS_ROUNDS];
+#pragma unroll
     for (int r = 0; r < RS_ROUNDS; r++) {
-        for (int w = 0; w < RS_WARPS; w++) warp_cnt[w][threadIdx.x] = 0;
-        __syncthreads();
-        const int64_t i = base + (int64_t)r * RS_BLOCK + threadIdx.x;
+        const int64_t i = base + r * 32 + lane;
         const bool valid = i < n;
-        uint64_t k = 0;
-        uint32_t v = 0;
-        int d = 256 + lane; // invalid lanes never match a real digit
-        if (valid) {
-            k = kin[i];
-            v = vin[i];
-            d = (int)((k >> shift) & 0xff);
+        const uint64_t k = valid ? kin[i] : 0;
+        const int d = valid ? (int)((k >> shift) & 0xff) : 256 + lane;
+        const unsigned peers = __match_any_sync(full, d);
+        const int before = valid ? S.warp_cnt[warp][d] : 0;
+        loc[r] = before + __popc(peers & lt_mask);
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) S.warp_cnt[warp][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // 2. thread t owns digit t: exclusive prefix over the warps, then over the digits
+    int32_t run = 0;
+    for (int w = 0; w < RS_WARPS; w++) {
+        const int32_t c = S.warp_cnt[w][threadIdx.x];
+        S.warp_cnt[w][threadIdx.x] = run;
+        run += c;
+    }
+    int32_t incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(full, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) S.wsum[warp] = incl;
+    __syncthreads();
+    int32_t wpre = 0;
+    for (int w = 0; w < warp; w++) wpre += S.wsum[w];
+    S.tile_start[threadIdx.x] = wpre + incl - run;
+    __syncthreads();
+    // 3. the tile in digit order, in shared memory (keys re-read: they are in L1/L2)
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; r++) {
+        const int64_t i = base + r * 32 + lane;
+        if (i < n) {
+            const uint64_t k = kin[i];
+            const int d = (int)((k >> shift) & 0xff);
+            const int sp = S.tile_start[d] + S.warp_cnt[warp][d] + loc[r];
+            S.sk[sp] = k;
+            S.sv[sp] = vin[i];
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        const int rank_in_warp = __popc(peers & lt_mask);
-        if (valid && rank_in_warp == 0) warp_cnt[warp][d] = __popc(peers);
-        __syncthreads();
-        // per digit: exclusive prefix over warps; thread t owns digit t
-        {
-            int32_t run = 0;
-            for (int w = 0; w < RS_WARPS; w++) {
-                const int32_t c = warp_cnt[w][threadIdx.x];
-                warp_cnt[w][threadIdx.x] = run;
-                run += c;
-            }
-            // stash the round total in the last slot pattern: add after ranks are read
-            __syncthreads();
-            if (valid) {
-                const int64_t dst = digit_base[d] + warp_cnt[warp][d] + rank_in_warp;
-                kout[dst] = k;
-                vout[dst] = v;
-            }
-            __syncthreads();
-            digit_base[threadIdx.x] += run;
-        }
-        __syncthreads();
+    }
+    __syncthreads();
+    // 4. out in order: consecutive threads write consecutive elements of a digit's run
+    const int cnt = (int)min((int64_t)RS_TILE, n - tile0);
+    for (int sp = threadIdx.x; sp < cnt; sp += RS_BLOCK) {
+        const uint64_t kk = S.sk[sp];
+        const int d = (int)((kk >> shift) & 0xff);
+        const int64_t dst = S.digit_base[d] + (sp - S.tile_start[d]);
+        kout[dst] = kk;
+        vout[dst] = S.sv[sp];
     }
 }
 
@@ -245,6 +288,12 @@ __global__ void k_radix_scatter(const uint64_t *__restrict__ kin, const uint32_t
 
 void vg_radix_sort_pairs(vg_ctx *ctx, uint64_t *keys, uint32_t *vals, int64_t n, int bits) {
     if (n <= 1 || bits <= 0) return;
+    static bool configured = false;
+    if (!configured) {
+        VG_CUDA(cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(RadixSmem)));
+        configured = true;
+    }
     const int64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
     DevBuf<uint64_t> k2(ctx, n);
     DevBuf<uint32_t> v2(ctx, n);
@@ -263,7 +312,7 @@ void vg_radix_sort_pairs(vg_ctx *ctx, uint64_t *keys, uint32_t *vals, int64_t n,
         vg_scan_i32_async(ctx, counts.p, offsets.p, 256 * ntiles, nullptr);
         {
             LaunchTimer lt(ctx);
-            k_radix_scatter<<<(unsigned)ntiles, RS_BLOCK, 0, ctx->stream>>>(
+            k_radix_scatter<<<(unsigned)ntiles, RS_BLOCK, sizeof(RadixSmem), ctx->stream>>>(
                 ka, va, kb, vb, n, shift, offsets.p, ntiles);
         }
         VG_CHECK_LAUNCH();
