@@ -64,7 +64,10 @@ __device__ __forceinline__ void store_relaxed(int32_t *p, int32_t v) {
 
 __global__ void __launch_bounds__(BFS_WARPS * 32) k_bfs_step(
     const int64_t *__restrict__ rowptr, const int32_t *__restrict__ tail, int64_t nv, int step,
-    int32_t *__restrict__ label, uint8_t *__restrict__ dist, unsigned long long *__restrict__ claimed) {
+    int32_t *__restrict__ label, uint8_t *__restrict__ dist, unsigned long long *__restrict__ claimed,
+    const unsigned long long *__restrict__ prev_claimed) {
+    // the level before claimed nothing: the search has ended, so has this level
+    if (prev_claimed && *prev_claimed == 0) return;
     __shared__ int32_t fl_all[BFS_WARPS][128];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -368,8 +371,8 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
     DevBuf<uint8_t> dist(ctx, nv);
     // steps run in groups of BFS_GROUP, each with its own claim counter, and the
     // counters are read back once per group: the search has ended at the first
-    // step that claimed nothing (the steps after it claim nothing either)
-    constexpr int BFS_GROUP = 4;
+    // step that claimed nothing (the steps after it see that count and return at once)
+    constexpr int BFS_GROUP = 8;
     DevBuf<unsigned long long> claimed(ctx, BFS_GROUP);
     unsigned long long *h =
         (unsigned long long *)vg_pinned(ctx, BFS_GROUP * sizeof(unsigned long long));
@@ -384,8 +387,9 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
         VG_CUDA(cudaMemsetAsync(claimed.p, 0, BFS_GROUP * sizeof(unsigned long long), ctx->stream));
         for (int k = 0; k < ns; k++) {
             LaunchTimer lt(ctx);
-            k_bfs_step<<<sgrid, BFS_WARPS * 32, 0, ctx->stream>>>(g->rowptr, g->tail, nv, step0 + k,
-                                                                 label.p, dist.p, claimed.p + k);
+            k_bfs_step<<<sgrid, BFS_WARPS * 32, 0, ctx->stream>>>(
+                g->rowptr, g->tail, nv, step0 + k, label.p, dist.p, claimed.p + k,
+                k > 0 ? claimed.p + k - 1 : nullptr);
             VG_CHECK_LAUNCH();
         }
         VG_CUDA(cudaMemcpyAsync(h, claimed.p, ns * sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
