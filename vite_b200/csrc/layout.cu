@@ -164,10 +164,12 @@ __global__ void __launch_bounds__(BFS_WARPS * 32) k_bfs_step(
 // degree bucket of the order key: the sweep's short-row kernels run each warp of
 // 32 consecutive vertices (the degree 17..32 kernel: 32 consecutive entries of its
 // position-ordered list) with loops as long as its largest row, so vertices of
-// similar degree are kept together inside a cluster (splitting 17..32 in three took
-// the RGG 2^24 run 53.3 -> 53.1 ms)
+// similar degree are kept together inside a cluster (RGG 2^24 run: buckets of width 4
+// up to 16 and one for 17..32: 53.3 ms; 17..32 split in three: 53.1 ms; widths 2 up to
+// 16 as well: 52.6 ms against 52.75)
 __device__ __forceinline__ uint32_t degree_bucket(int64_t d) {
-    return d <= 8 ? 0u : d <= 12 ? 1u : d <= 16 ? 2u : d <= 20 ? 3u : d <= 24 ? 4u : d <= 32 ? 5u : 6u;
+    return d <= 6 ? 0u : d <= 8 ? 1u : d <= 10 ? 2u : d <= 12 ? 3u : d <= 14 ? 4u : d <= 16 ? 5u
+         : d <= 20 ? 6u : d <= 24 ? 7u : d <= 32 ? 8u : 9u;
 }
 
 // (cluster, degree bucket, BFS distance), the distance in dbits bits; unreached
@@ -179,8 +181,8 @@ __global__ void k_order_keys(int64_t nv, const int64_t *__restrict__ rowptr,
          v += (int64_t)gridDim.x * blockDim.x) {
         const int32_t l = label[v];
         const uint64_t b = degree_bucket(rowptr[v + 1] - rowptr[v]);
-        keys[v] = l < 0 ? (((uint64_t)v << (3 + dbits)) | (7ull << dbits))
-                        : (((uint64_t)l << (3 + dbits)) | (b << dbits) | dist[v]);
+        keys[v] = l < 0 ? (((uint64_t)v << (4 + dbits)) | (15ull << dbits))
+                        : (((uint64_t)l << (4 + dbits)) | (b << dbits) | dist[v]);
         vals[v] = (uint32_t)v;
     }
 }
@@ -411,7 +413,7 @@ void vg_bfs_order(vg_ctx *ctx, const vg_graph *g, DevBuf<int32_t> &order) {
     VG_CHECK_LAUNCH();
     int vbits = 1;
     while (vbits < 40 && ((int64_t)1 << vbits) < nv) vbits++;
-    vg_radix_sort_pairs(ctx, keys.p, vals.p, nv, vbits + 3 + dbits);
+    vg_radix_sort_pairs(ctx, keys.p, vals.p, nv, vbits + 4 + dbits);
     VG_CUDA(cudaMemcpyAsync(order.p, vals.p, sizeof(int32_t) * nv, cudaMemcpyDeviceToDevice,
                             ctx->stream));
 }
