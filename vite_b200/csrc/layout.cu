@@ -12,7 +12,7 @@
 // reference's. Only the addresses change.
 //
 // The locality order is computed on the device from the graph alone: a
-// multi-source breadth-first search from hashed seeds (about one seed per 512
+// multi-source breadth-first search from hashed seeds (about one seed per 256
 // vertices) labels each vertex with its nearest seed, and vertices are ordered by
 // (seed, degree bucket, BFS distance, id), so a cluster occupies a contiguous range
 // of positions, most neighbours of a vertex lie in the same few cache lines, and
@@ -25,9 +25,10 @@ namespace {
 
 // one seed per 2^SEED_SHIFT vertices on average. Measured on RGG 2^24 (level-0 sweep
 // set / whole run): 2^12 25.4 / 57.9 ms, 2^11 23.8 / 56.0, 2^10 22.7 / 54.9, 2^9 22.2 /
-// 54.3, 2^8 22.3 / 54.1, 2^7 22.8 / 54.7, 2^6 23.4 / 55.3
+// 54.3, 2^8 22.3 / 54.1, 2^7 22.8 / 54.7, 2^6 23.4 / 55.3; with the current BFS and
+// degree buckets 2^10 22.8 / 53.5, 2^9 22.3 / 52.9, 2^8 22.3 / 52.8
 #ifndef VG_SEED_SHIFT
-#define VG_SEED_SHIFT 9
+#define VG_SEED_SHIFT 8
 #endif
 constexpr int SEED_SHIFT = VG_SEED_SHIFT;
 constexpr int MAX_BFS_STEPS = 255;
