@@ -94,14 +94,17 @@ def test_upload_download_roundtrip(ctx):
 # --------------------------------------------------------------------------------------
 # operators
 
-@pytest.mark.parametrize("maker", ["rgg", "ba", "hub", "star_big", "star_big_real"])
+@pytest.mark.parametrize("maker", ["rgg", "ba", "ba_real", "hub", "star_big", "star_big_real"])
 def test_vertex_degree(ctx, maker):
     """star_big: a 40,000-entry hub row, which integral weights sum in chunks over many
-    blocks (and real weights as one ordered fold)"""
+    blocks (and real weights as one ordered fold); ba_real: real-weight rows of 64 to a
+    few thousand entries, folded in order by a warp each"""
     if maker == "rgg":
         ref = vo.rgg(65536)
     elif maker == "ba":
         ref = vo.ba(20000, 8, 3)
+    elif maker == "ba_real":
+        ref = vo.reweight(vo.ba(20000, 8, 3), 2, 19)
     elif maker == "star_big":
         ref = star_graph(40001, 3.0)
     elif maker == "star_big_real":
@@ -304,17 +307,57 @@ def path_graph(n, seed):
                              np.concatenate([w, w]))
 
 
+def long_runs_graph(seed):
+    """Real-weight groups joined completely in pairs (A, B): the rebuilt row of A holds
+    one run of |A| x |B| entries for B, of 129 to 6,000 entries (just above the
+    thread-per-run limit, at and around one staging step of 256, many steps). Every
+    group vertex also has enough random edges into 20-vertex filler communities that
+    the row of A has more distinct neighbours than the shared-memory tables hold, so
+    it takes the sorted path. Returns (graph, communities)."""
+    rng = np.random.default_rng(seed)
+    pairs = [(3, 43), (10, 13), (16, 16), (257, 1), (1, 257), (100, 60), (7, 41)]
+    n = 20000
+    cv = np.empty(n, np.int64)
+    src, dst = [], []
+    nxt = 0
+    groups = []
+    for a, b in pairs:
+        A = np.arange(nxt, nxt + a)
+        B = np.arange(nxt + a, nxt + a + b)
+        nxt += a + b
+        cv[A] = A[0]
+        cv[B] = B[0]
+        groups += [A, B]
+        src.append(np.repeat(A, b))
+        dst.append(np.tile(B, a))
+    filler = np.arange(nxt, n)
+    cv[filler] = nxt + (filler - nxt) // 20 * 20
+    for G in groups:
+        r = -(-400 // len(G))
+        src.append(np.repeat(G, r))
+        dst.append(rng.choice(filler, len(G) * r))
+    a = np.concatenate(src)
+    b = np.concatenate(dst)
+    w = rng.random(len(a))
+    g = vo._csr_from_list(n, np.concatenate([a, b]), np.concatenate([b, a]),
+                          np.concatenate([w, w]))
+    return g, cv
+
+
 @pytest.mark.parametrize("layout", [0, 1])
 @pytest.mark.parametrize("case", ["one_community", "blocks_of_600", "random_blocks",
-                                  "ba_blocks_of_12", "isolated_members", "path_blocks_of_300"])
+                                  "ba_blocks_of_12", "isolated_members", "path_blocks_of_300",
+                                  "long_runs"])
 def test_rebuild_segment_classes(ctx, case, layout):
     """Next-level segments of every size class: the warp hash path (<=256 entries, with
     at most 32 or more distinct neighbours) and the global sorted path (longer), with
-    real weights folded in order. The warp tables read each segment from its members'
+    real weights folded in order (long runs by a warp each: long_runs). The warp tables read each segment from its members'
     rows through windows of 32 members: segments of hundreds of short rows slide the
     window, and members without entries (isolated vertices put into communities by
     the caller) leave gaps inside it."""
-    if case == "isolated_members":
+    if case == "long_runs":
+        gref, cv = long_runs_graph(31)
+    elif case == "isolated_members":
         gref = with_isolated(vo.reweight(vo.rgg(16384), 2, 13), 3000)
         cv = ((np.arange(gref.nv) * 7919) % 250 * 3).astype(np.int64)
     elif case == "path_blocks_of_300":

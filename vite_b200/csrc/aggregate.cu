@@ -396,6 +396,8 @@ __global__ void k_big_rowmap(int64_t nc, const int32_t *__restrict__ flag,
 
 constexpr int BIG_CHUNK = 4096;
 constexpr int64_t BIG_RUN_LONG = 1024; // integral weights: longer runs are folded by a warp
+constexpr int64_t SEQ_RUN = 128;       // real weights: longer runs go to k_big_fold_seq
+constexpr int SEQ_WARPS = 4;           // warps per k_big_fold_seq block
 
 // per segment r: its length and chunk count when flagged (more distinct keys than
 // the warp table holds), else 0
@@ -456,21 +458,22 @@ __global__ void k_big_rowfirst(const uint64_t *__restrict__ K, int64_t m, int kb
 }
 
 // one thread per run: the run's bounds are known, so its weights are fetched
-// eight at a time ahead of the strictly ordered additions
+// eight at a time ahead of the strictly ordered additions; runs longer than
+// run_long entries are listed for a warp each (k_big_fold_long, k_big_fold_seq)
 __global__ void k_big_fold(const uint64_t *__restrict__ K, const uint32_t *__restrict__ V, int64_t m,
                            int kbits, const int64_t *__restrict__ nheads_dev,
                            const int64_t *__restrict__ headpos,
                            const int64_t *__restrict__ rowfirst, const int32_t *__restrict__ big_row,
                            const int64_t *__restrict__ rstart, const double *__restrict__ gw,
                            int32_t *__restrict__ uk, double *__restrict__ uw,
-                           int64_t *__restrict__ long_runs, int64_t long_cap,
+                           int64_t *__restrict__ long_runs, int64_t long_cap, int64_t run_long,
                            unsigned long long *__restrict__ long_count) {
     const uint64_t mask = ((uint64_t)1 << kbits) - 1;
     const int64_t nheads = *nheads_dev;
     for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nheads;
          h += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i0 = headpos[h], i1 = h + 1 < nheads ? headpos[h + 1] : m;
-        if (long_runs && i1 - i0 > BIG_RUN_LONG) { // listed for k_big_fold_long
+        if (long_runs && i1 - i0 > run_long) {
             const unsigned long long sl = atomicAdd(long_count, 1ULL);
             if ((int64_t)sl < long_cap) long_runs[sl] = h;
             continue;
@@ -533,6 +536,37 @@ __global__ void k_big_fold_long(const uint64_t *__restrict__ K, const uint32_t *
             const int64_t o = rstart[big_row[q]] + (h - rowfirst[q]);
             uk[o] = (int32_t)(k & mask);
             uw[o] = sum;
+        }
+    }
+}
+
+// real weights: the listed runs (longer than SEQ_RUN entries), one warp each; the
+// sum stays one left fold in run order (vg_warp_ordered_fold)
+__global__ void k_big_fold_seq(
+    const uint64_t *__restrict__ K, const uint32_t *__restrict__ V, int64_t m, int kbits,
+    const int64_t *__restrict__ nheads_dev, const int64_t *__restrict__ headpos,
+    const int64_t *__restrict__ rowfirst, const int32_t *__restrict__ big_row,
+    const int64_t *__restrict__ rstart, const double *__restrict__ gw, int32_t *__restrict__ uk,
+    double *__restrict__ uw, const int64_t *__restrict__ long_runs, int64_t long_cap,
+    const unsigned long long *__restrict__ long_count) {
+    __shared__ double stage[SEQ_WARPS][2 * VG_FOLD_STEP];
+    const uint64_t mask = ((uint64_t)1 << kbits) - 1;
+    const int64_t nheads = *nheads_dev;
+    const int64_t nl = min((int64_t)*long_count, long_cap);
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < nl; r += nw) {
+        const int64_t h = long_runs[r];
+        const int64_t i0 = headpos[h], i1 = h + 1 < nheads ? headpos[h + 1] : m;
+        const double *__restrict__ sw = gw + rstart[big_row[K[i0] >> kbits]]; // segment's weights
+        const uint32_t *__restrict__ rv = V + i0;
+        const double s = vg_warp_ordered_fold(
+            i1 - i0, [sw, rv](int64_t j) { return sw[rv[j]]; }, stage[threadIdx.x >> 5], 0.0, true);
+        if ((threadIdx.x & 31) == 0) { // the run's key and place read again: fewer live values
+            const uint64_t k = K[i0];
+            const uint64_t q = k >> kbits;
+            const int64_t o = rstart[big_row[q]] + (h - rowfirst[q]);
+            uk[o] = (int32_t)(k & mask);
+            uw[o] = s;
         }
     }
 }
@@ -770,22 +804,30 @@ vg_graph *vg_aggregate_rows(vg_ctx *ctx, const vg_graph *g, const int32_t *pos,
                                                                             rowfirst.p, headpos.p); }
             VG_CHECK_LAUNCH();
             hr.release();
-            // integral weights: runs longer than BIG_RUN_LONG are listed for a warp each
-            const int64_t lcap = integral ? m / (BIG_RUN_LONG + 1) + 1 : 0;
+            // runs longer than run_long entries are listed for a warp each: integral
+            // weights sum them in any order (k_big_fold_long), real weights in order
+            // (k_big_fold_seq)
+            const int64_t run_long = integral ? BIG_RUN_LONG : SEQ_RUN;
+            const int64_t lcap = m / (run_long + 1) + 1;
             DevBuf<int64_t> lruns(ctx, lcap);
-            DevBuf<unsigned long long> lcount(ctx, integral ? 1 : 0);
-            if (integral)
-                VG_CUDA(cudaMemsetAsync(lcount.p, 0, sizeof(unsigned long long), ctx->stream));
+            DevBuf<unsigned long long> lcount(ctx, 1);
+            VG_CUDA(cudaMemsetAsync(lcount.p, 0, sizeof(unsigned long long), ctx->stream));
             { LaunchTimer lt(ctx);
               k_big_fold<<<vg_grid(ctx, m, 128), 128, 0, ctx->stream>>>(
                   K.p, V.p, m, kbits, tot.p + 3, headpos.p, rowfirst.p, big_row.p, rstart.p, gw.p,
-                  uk.p, uw.p, lruns.p, lcap, lcount.p); }
+                  uk.p, uw.p, lruns.p, lcap, run_long, lcount.p); }
             VG_CHECK_LAUNCH();
             if (integral) {
                 LaunchTimer lt(ctx);
                 k_big_fold_long<<<vg_grid(ctx, lcap * 32, 256), 256, 0, ctx->stream>>>(
                     K.p, V.p, m, kbits, tot.p + 3, headpos.p, rowfirst.p, big_row.p, rstart.p, gw.p,
                     uk.p, uw.p, lruns.p, lcap, lcount.p);
+            } else {
+                LaunchTimer lt(ctx);
+                k_big_fold_seq<<<vg_grid(ctx, lcap * 32, SEQ_WARPS * 32), SEQ_WARPS * 32, 0,
+                                 ctx->stream>>>(K.p, V.p, m, kbits, tot.p + 3, headpos.p,
+                                                rowfirst.p, big_row.p, rstart.p, gw.p, uk.p, uw.p,
+                                                lruns.p, lcap, lcount.p);
             }
             VG_CHECK_LAUNCH();
             { LaunchTimer lt(ctx);

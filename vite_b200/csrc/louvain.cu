@@ -1412,13 +1412,14 @@ __global__ void k_degree_huge(const int64_t *__restrict__ rowptr, const double *
 
 // one warp per listed row. Integral weights: every partial sum is exact, so lanes
 // add strided entries and a shuffle tree combines them. Otherwise the row's left
-// fold in CSR order: the warp loads 32 consecutive weights (the next 32 in flight
-// meanwhile) and every lane adds them in lane order from broadcasts, so all lanes
-// hold the serial fold's bits.
-__global__ void k_degree_long(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
+// fold in CSR order (vg_warp_ordered_fold: the warp fetches the weights ahead of
+// lane 0's chain of additions).
+constexpr int DEG_LONG_WARPS = 8; // warps per k_degree_long block
+__global__ void __launch_bounds__(DEG_LONG_WARPS * 32) k_degree_long(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
                               double *__restrict__ vdeg, const int32_t *__restrict__ long_rows,
                               int64_t long_cap, const unsigned long long *__restrict__ long_count,
                               int integral) {
+    __shared__ double stage[DEG_LONG_WARPS][2 * VG_FOLD_STEP];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int64_t n = min((int64_t)*long_count, long_cap);
@@ -1443,18 +1444,10 @@ __global__ void k_degree_long(const int64_t *__restrict__ rowptr, const double *
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) sum = __dadd_rn(sum, __shfl_xor_sync(full, sum, o));
         } else {
-            double x = E0 + lane < E1 ? w[E0 + lane] : 0.0;
-            for (int64_t base = E0; base < E1; base += 32) {
-                const int64_t kn = base + 32 + lane;
-                const double xn = kn < E1 ? w[kn] : 0.0;
-                const int cnt = (int)min((int64_t)32, E1 - base);
-#pragma unroll
-                for (int j = 0; j < 32; j++) {
-                    const double y = __shfl_sync(full, x, j);
-                    if (j < cnt) sum = __dadd_rn(sum, y);
-                }
-                x = xn;
-            }
+            // real weights: one left fold in CSR order (lane 0's result)
+            const double *__restrict__ rw = w + E0;
+            sum = vg_warp_ordered_fold(E1 - E0, [rw](int64_t j) { return rw[j]; },
+                                       stage[threadIdx.x >> 5], 0.0, false);
         }
         if (lane == 0) vdeg[v] = sum;
     }
@@ -2031,7 +2024,8 @@ static void vertex_degrees(vg_ctx *ctx, const vg_graph *g, double *vdeg, int int
     }
     if (g->ne > DEG_LONG) {
         LaunchTimer lt(ctx);
-        k_degree_long<<<vg_grid(ctx, cap * 32, 256, 8), 256, 0, ctx->stream>>>(
+        k_degree_long<<<vg_grid(ctx, cap * 32, DEG_LONG_WARPS * 32, 8), DEG_LONG_WARPS * 32, 0,
+                        ctx->stream>>>(
             g->rowptr, g->weight, vdeg, list.p, cap, cnt.p, integral);
     }
     VG_CHECK_LAUNCH();

@@ -236,6 +236,61 @@ __device__ __forceinline__ double vg_fold_above(double acc, const double *stage,
     return acc;
 }
 
+// One left fold of n values, get(0) .. get(n - 1) in that order, by a whole warp:
+// lane 0 returns s + get(0) + ... + get(n - 1) added one at a time (with first, the
+// fold starts from get(0) instead of s + get(0)). The additions are one chain of
+// dependent operations, so the warp only keeps that chain fed: all lanes fetch the
+// next VG_FOLD_STEP values into registers while lane 0 adds the current ones from
+// `stage`, the warp's own 2 x VG_FOLD_STEP doubles of shared memory. A stage is
+// rewritten only after the __syncwarp that follows lane 0's reads of it; the final
+// __syncwarp lets the caller reuse `stage` at once. n, s and first are warp-uniform.
+constexpr int VG_FOLD_STEP = 256;
+template <class Get>
+__device__ __forceinline__ double vg_warp_ordered_fold(int64_t n, Get get, double *stage,
+                                                       double s, bool first) {
+    constexpr int PER = VG_FOLD_STEP / 32;
+    const int lane = threadIdx.x & 31;
+    double x[PER];
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        const int64_t j = t * 32 + lane;
+        x[t] = j < n ? get(j) : 0.0;
+    }
+    int b = 0;
+    for (int64_t c0 = 0; c0 < n; c0 += VG_FOLD_STEP, b ^= 1) {
+        double *st = stage + b * VG_FOLD_STEP;
+#pragma unroll
+        for (int t = 0; t < PER; t++) st[t * 32 + lane] = x[t];
+        __syncwarp();
+        const int64_t c1 = c0 + VG_FOLD_STEP;
+        if (c1 < n) { // the next step's values, in flight during the additions
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                const int64_t j = c1 + t * 32 + lane;
+                x[t] = j < n ? get(j) : 0.0;
+            }
+        }
+        if (lane == 0) {
+            const int cnt = (int)(n - c0 < VG_FOLD_STEP ? n - c0 : VG_FOLD_STEP);
+            int t = 0;
+            if (first && c0 == 0) {
+                s = st[0];
+                t = 1;
+            }
+            for (; t + 8 <= cnt; t += 8) {
+                double y[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) y[u] = st[t + u];
+#pragma unroll
+                for (int u = 0; u < 8; u++) s = __dadd_rn(s, y[u]);
+            }
+            for (; t < cnt; t++) s = __dadd_rn(s, st[t]);
+        }
+    }
+    __syncwarp();
+    return s;
+}
+
 // counter-based generator shared with the oracle's restatement
 __host__ __device__ __forceinline__ uint64_t vg_sm64(uint64_t x) {
     x += 0x9E3779B97F4A7C15ULL;
