@@ -277,10 +277,21 @@ __device__ __forceinline__ double vg_warp_ordered_fold(int64_t n, Get get, doubl
                 s = st[0];
                 t = 1;
             }
-            for (; t + 8 <= cnt; t += 8) {
+            if (t + 8 <= cnt) {
+                // the next eight values are read before the current eight are added,
+                // so the chain waits on the additions only
                 double y[8];
 #pragma unroll
                 for (int u = 0; u < 8; u++) y[u] = st[t + u];
+                for (t += 8; t + 8 <= cnt; t += 8) {
+                    double z[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) z[u] = st[t + u];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) s = __dadd_rn(s, y[u]);
+#pragma unroll
+                    for (int u = 0; u < 8; u++) y[u] = z[u];
+                }
 #pragma unroll
                 for (int u = 0; u < 8; u++) s = __dadd_rn(s, y[u]);
             }
