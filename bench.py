@@ -461,48 +461,26 @@ def serving_workload(ctx, count: int, seed: int):
     return hosts, kinds, base
 
 
-def serving_bound(service: list, visits: list, ne: list, kinds=None) -> dict:
+def serving_bound(service: list, visits: list, ne: list) -> dict:
     """What batching can gain on this mix at most. A request's plain service time t_i
     cannot shrink below what its own edge visits (sum over levels of entries x
     iterations) cost at the best rate any request reached alone, R = max_i v_i / t_i;
     requests that already run within 20 % of R alone (the large ones: they fill the GPU
     by themselves) keep their own time. T_served >= sum_sat t_i + sum_other v_i / R, so
-    served/plain throughput <= sum t_i / that.
-
-    With kinds (graph family per request), `by_family` applies the same rule with R
-    taken per family: an edge visit of a Barabasi-Albert graph (no locality layout,
-    skewed degrees) costs more than one of an RGG at any size, and batching does not
-    change what a visit of its family costs."""
+    served/plain throughput <= sum t_i / that."""
     t = np.asarray(service, dtype=np.float64)
     v = np.asarray(visits, dtype=np.float64)
     rate = v / t
     R = float(rate.max())
     sat = rate >= 0.8 * R
     floor_ = float(t[sat].sum() + (v[~sat] / R).sum())
-    out = {"peak_rate_edge_visits_per_s": R, "saturating_requests": int(sat.sum()),
-           "saturating_min_entries": int(np.asarray(ne)[sat].min()) if sat.any() else None,
-           "plain_time_share_of_saturating": float(t[sat].sum() / t.sum()),
-           "min_served_seconds": floor_, "max_speedup": float(t.sum() / floor_),
-           "rule": "T_served >= sum(t_i, requests within 20% of the best rate R alone) + "
-                   "sum(visits_i / R, the others); visits = sum over levels of entries x "
-                   "iterations; t_i = plain service time with the upload"}
-    if kinds is not None:
-        fam = np.asarray(kinds)
-        names = {0: "rgg", 1: "ba"}
-        floor_f, peaks, nsat = 0.0, {}, 0
-        for k in np.unique(fam):
-            m = fam == k
-            Rk = float(rate[m].max())
-            sk = m & (rate >= 0.8 * Rk)
-            floor_f += float(t[sk].sum() + (v[m & ~sk] / Rk).sum())
-            peaks[names.get(int(k), str(k))] = Rk
-            nsat += int(sk.sum())
-        out["by_family"] = {"peak_rate_edge_visits_per_s": peaks, "saturating_requests": nsat,
-                            "min_served_seconds": floor_f,
-                            "max_speedup": float(t.sum() / floor_f),
-                            "rule": "the same rule with R the best rate of the request's own "
-                                    "graph family alone"}
-    return out
+    return {"peak_rate_edge_visits_per_s": R, "saturating_requests": int(sat.sum()),
+            "saturating_min_entries": int(np.asarray(ne)[sat].min()) if sat.any() else None,
+            "plain_time_share_of_saturating": float(t[sat].sum() / t.sum()),
+            "min_served_seconds": floor_, "max_speedup": float(t.sum() / floor_),
+            "rule": "T_served >= sum(t_i, requests within 20% of the best rate R alone) + "
+                    "sum(visits_i / R, the others); visits = sum over levels of entries x "
+                    "iterations; t_i = plain service time with the upload"}
 
 
 def run_serving(ctx, count: int, lanes=SERVE_LANES) -> dict:
@@ -528,7 +506,7 @@ def run_serving(ctx, count: int, lanes=SERVE_LANES) -> dict:
     agree = sum(levels_agree(s.levels, p.levels) for s, p in zip(served.results, plain.results))
     gps = count / served.seconds
     plain_gps = count / float(fin.max() - arrivals.min())
-    bound = serving_bound(service, visits, ne, kinds)
+    bound = serving_bound(service, visits, ne)
     del hosts
     return {
         "workload": f"{count} requests, CSR entries log-uniform [{SERVE_E[0]:g}, {SERVE_E[1]:g}], "
@@ -552,7 +530,6 @@ def run_serving(ctx, count: int, lanes=SERVE_LANES) -> dict:
                  "queue over those service times",
         "bound": bound,
         "fraction_of_bound": (gps / plain_gps) / bound["max_speedup"],
-        "fraction_of_bound_by_family": (gps / plain_gps) / bound["by_family"]["max_speedup"],
         "agree_with_plain": f"{agree}/{count} requests: same levels, per-level modularity within "
                             f"{REL_TOL:g} relative",
     }
