@@ -1414,11 +1414,12 @@ __global__ void k_degree_huge(const int64_t *__restrict__ rowptr, const double *
 // add strided entries and a shuffle tree combines them. Otherwise the row's left
 // fold in CSR order (vg_warp_ordered_fold: the warp fetches the weights ahead of
 // lane 0's chain of additions).
-constexpr int DEG_LONG_WARPS = 8; // warps per k_degree_long block
-__global__ void __launch_bounds__(DEG_LONG_WARPS * 32) k_degree_long(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
-                              double *__restrict__ vdeg, const int32_t *__restrict__ long_rows,
-                              int64_t long_cap, const unsigned long long *__restrict__ long_count,
-                              int integral) {
+constexpr int DEG_LONG_WARPS = 4; // warps per k_degree_long block (one chain per scheduler)
+__global__ void __launch_bounds__(DEG_LONG_WARPS * 32)
+    k_degree_long(const int64_t *__restrict__ rowptr, const double *__restrict__ w,
+                  double *__restrict__ vdeg, const int32_t *__restrict__ long_rows,
+                  int64_t long_cap, const unsigned long long *__restrict__ long_count,
+                  int integral) {
     __shared__ double stage[DEG_LONG_WARPS][2 * VG_FOLD_STEP];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;

@@ -278,22 +278,35 @@ __device__ __forceinline__ double vg_warp_ordered_fold(int64_t n, Get get, doubl
                 t = 1;
             }
             if (t + 8 <= cnt) {
-                // the next eight values are read before the current eight are added,
-                // so the chain waits on the additions only
-                double y[8];
+                // groups of eight, alternately in ya and yb: the next group is read
+                // before the current one is added, so the chain waits on the
+                // additions only
+                double ya[8], yb[8];
 #pragma unroll
-                for (int u = 0; u < 8; u++) y[u] = st[t + u];
-                for (t += 8; t + 8 <= cnt; t += 8) {
-                    double z[8];
+                for (int u = 0; u < 8; u++) ya[u] = st[t + u];
+                t += 8;
+                for (;;) {
+                    if (t + 8 > cnt) {
 #pragma unroll
-                    for (int u = 0; u < 8; u++) z[u] = st[t + u];
+                        for (int u = 0; u < 8; u++) s = __dadd_rn(s, ya[u]);
+                        break;
+                    }
 #pragma unroll
-                    for (int u = 0; u < 8; u++) s = __dadd_rn(s, y[u]);
+                    for (int u = 0; u < 8; u++) yb[u] = st[t + u];
+                    t += 8;
 #pragma unroll
-                    for (int u = 0; u < 8; u++) y[u] = z[u];
+                    for (int u = 0; u < 8; u++) s = __dadd_rn(s, ya[u]);
+                    if (t + 8 > cnt) {
+#pragma unroll
+                        for (int u = 0; u < 8; u++) s = __dadd_rn(s, yb[u]);
+                        break;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) ya[u] = st[t + u];
+                    t += 8;
+#pragma unroll
+                    for (int u = 0; u < 8; u++) s = __dadd_rn(s, yb[u]);
                 }
-#pragma unroll
-                for (int u = 0; u < 8; u++) s = __dadd_rn(s, y[u]);
             }
             for (; t < cnt; t++) s = __dadd_rn(s, st[t]);
         }
