@@ -58,14 +58,15 @@ constexpr int64_t NA_LONG = 64;
 
 // one block per tile: each row summed in CSR order (as distSumVertexDegree), and
 // the tile's degrees reduced into its partial. A lane folds its own row when it is
-// short; the warp's long rows (hubs) are folded one after another by all its lanes,
-// 32 consecutive weights loaded at a time and added in lane order from broadcasts,
-// so every lane holds the serial fold's bits and a hub costs its length / 32 steps
+// short; the warp's long rows (hubs) are folded one after another by all its lanes
+// (vg_warp_ordered_fold: the lanes fetch the row's weights ahead of lane 0's chain of
+// additions, in static shared memory), so a hub costs one addition per entry
 __global__ void __launch_bounds__(NA_THREADS) k_na_degree(const int64_t *__restrict__ rowptr,
                                                           const double *__restrict__ w, int64_t nv,
                                                           double *__restrict__ vdeg,
                                                           double *__restrict__ partial) {
     __shared__ double ws[32];
+    __shared__ double stage[NA_THREADS / 32][2 * VG_FOLD_STEP];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     double s = 0.0;
@@ -86,16 +87,10 @@ __global__ void __launch_bounds__(NA_THREADS) k_na_degree(const int64_t *__restr
         for (unsigned lm = __ballot_sync(full, lng); lm; lm &= lm - 1) {
             const int src = __ffs(lm) - 1;
             const int64_t E0 = __shfl_sync(full, e0, src), E1 = __shfl_sync(full, e1, src);
-            double acc = 0.0;
-            for (int64_t b = E0; b < E1; b += 32) {
-                const double x = b + lane < E1 ? w[b + lane] : 0.0;
-                const int cnt = (int)min((int64_t)32, E1 - b);
-#pragma unroll
-                for (int j = 0; j < 32; j++) {
-                    const double y = __shfl_sync(full, x, j);
-                    if (j < cnt) acc = __dadd_rn(acc, y);
-                }
-            }
+            const double *__restrict__ rw = w + E0;
+            double acc = vg_warp_ordered_fold(E1 - E0, [rw](int64_t j) { return rw[j]; },
+                                              stage[threadIdx.x >> 5], 0.0, false);
+            acc = __shfl_sync(full, acc, 0); // lane 0 holds the fold
             if (lane == src) tw = acc;
         }
         if (valid) {
