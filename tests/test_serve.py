@@ -9,11 +9,6 @@ from vite_b200 import serve as sv
 pytestmark = pytest.mark.gpu
 
 
-def test_fifo_finish_times():
-    fin = sv.fifo([0.0, 0.1, 5.0], [1.0, 1.0, 1.0])
-    assert list(fin) == [1.0, 2.0, 6.0]
-
-
 @pytest.mark.parametrize("lanes", [(), (20000,)])
 def test_served_results_equal_alone(ctx, lanes):
     gs = []
